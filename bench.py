@@ -1,0 +1,424 @@
+"""Benchmark of the cuCOSMA-compatible GEMM library on B200.
+
+Workload (single GPU): the precision forms at M = N = K = 8192, alpha = 1,
+beta = 0, entries i.i.d. uniform[-1, 1] from fixed seeds (synthetic; the
+reference uses no dataset).  The headline "step" is one FP32 SGEMM through
+the BF16x3 tensor-core path (split pre-pass + tcgen05 GEMM); the same
+protocol times the native FP32 (FFMA) SGEMM, the native FP64 (DFMA) DGEMM
+and the Ozaki INT8-slice DGEMM, each reported with TFLOP/s, % of its
+relevant peak and its error against an FP64 (double-double for FP64 paths)
+CPU oracle evaluated on a sample of rows.
+
+Timing: W untimed warm-up steps, then exactly K steps bracketed by a
+barrier and torch.cuda.synchronize(), CUDA events on the launching stream,
+max over ranks.  Every input is larger than the 126 MB L2 (256 MB per FP32
+operand), so no flush is needed between steps.
+
+--impl reference times the reference's own CPU product
+(Matrix<double>::operator*, Kernel/cuda/src/Matrix.h:183-201, built from its
+sources into oracle/_ref/) on a bounded sample of rows of the same workload,
+on all host threads.
+
+Multi-GPU: the path does not shard (one GEMM per GPU); --gpus N runs N
+independent replicas, one per rank, and reports the aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TFLOP/s & % of peak: BF16x3/Ozaki vs native S/DGEMM at stated error vs FP64"
+OZAKI_SLICES = 8
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return {"bf16": float(p["bf16_tflops"]), "bf16_sustained": float(p.get("bf16_tflops_sustained", 0) or 0),
+                "hbm": float(p["hbm_gbs"]), "sm_max_mhz": float(p.get("sm_max_mhz", 1965.0)), "source": "measured"}
+    except Exception:
+        return {"bf16": 1590.0, "bf16_sustained": 1400.0, "hbm": 6650.0, "sm_max_mhz": 1965.0, "source": "fallback"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) of SM clock and throttle reasons."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(n_gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- workload
+def make_inputs(n, seed, dtype):
+    import torch
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    return torch.rand((n, n), generator=g, device="cuda", dtype=dtype) * 2 - 1
+
+
+def time_path(cc, A, B, Cm, prec, slices, steps, warmup, world, workspace):
+    """Average ms per call over exactly `steps` calls (device events), plus the
+    main kernel's average ms and the library launch count in the timed region."""
+    import torch
+
+    kw = dict(precision=prec, slices=slices, workspace=workspace)
+    for _ in range(warmup):
+        cc.gemm(A, B, Cm, 1.0, 0.0, **kw)
+    st = torch.cuda.current_stream()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = cc.launch_count()
+    cc.profile_start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        cc.gemm(A, B, Cm, 1.0, 0.0, **kw)
+    e1.record(st)
+    barrier(world)
+    torch.cuda.synchronize()
+    kern_ms, kern_n = cc.profile_stop()
+    launches = cc.launch_count() - l0
+    ms = e0.elapsed_time(e1) / steps
+    return ms, (kern_ms / kern_n if kern_n else None), launches
+
+
+def e2e_path(cc, A_h, B_h, C_h, A, B, Cm, prec, slices, steps, warmup, workspace):
+    """Same metric through the public call with host buffers: pinned H2D of
+    A and B, the GEMM, D2H of C, all inside the timed region."""
+    import torch
+
+    st = torch.cuda.current_stream()
+
+    def one():
+        A.copy_(A_h, non_blocking=True)
+        B.copy_(B_h, non_blocking=True)
+        cc.gemm(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices, workspace=workspace)
+        C_h.copy_(Cm, non_blocking=True)
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        one()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+# -------------------------------------------------------------- CPU legs
+def cpu_sample(n, A32, B32, A64, B64, outs, budget_s=12.0):
+    """CPU baseline leg: times the FP64 oracle on a bounded sample of rows of
+    the FP32 workload (all host threads) and uses the same rows -- plus a
+    double-double sample of the FP64 workload -- as the checker that states
+    the error of each GPU result.  Returns (cpu_baseline, errors)."""
+    import oracle
+
+    threads = oracle.lib().oracle_max_threads()
+    rows_probe = 8
+    t0 = time.perf_counter()
+    oracle.gemm(A32[:rows_probe], B32, threads=threads)
+    dt = time.perf_counter() - t0
+    rows = int(max(rows_probe, min(n, rows_probe * budget_s / max(dt, 1e-3))))
+    rows = max(rows_probe, min(rows, 1024))
+    idx = np.linspace(0, n - 1, rows).astype(np.int64)
+    t0 = time.perf_counter()
+    ref32 = oracle.gemm(A32[idx], B32, threads=threads)
+    dt = time.perf_counter() - t0
+    tflops = 2.0 * rows * n * n / dt / 1e12
+    cpu = {"value": tflops, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+           "sample": "FP64 oracle (Matrix.h:183-201 order, OpenMP over rows) on %d of %d rows of the %d^3 FP32 "
+                     "workload, %.1f s" % (rows, n, n, dt)}
+    errs = {}
+    for name, out in outs.items():
+        if out is None:
+            continue
+        if out.dtype == np.float32:
+            errs[name] = oracle.errors(out[idx], ref32)
+    # FP64 paths: double-double reference on a few rows of the FP64 workload.
+    r64 = np.linspace(0, n - 1, 8).astype(np.int64)
+    hi, lo = oracle.gemm(A64[r64], B64, dd=True, threads=threads)
+    for name, out in outs.items():
+        if out is not None and out.dtype == np.float64:
+            errs[name] = oracle.errors(out[r64], hi, lo)
+    return cpu, errs
+
+
+def reference_arm(args):
+    """--impl reference: the reference's own CPU product on host threads."""
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = args.size
+    import oracle
+
+    rng = np.random.default_rng(1)
+    threads = os.cpu_count() or 1
+    rows_per_thread = max(1, args.ref_rows // threads)
+    rows = rows_per_thread * threads
+    B = rng.uniform(-1, 1, (n, n))
+    A = rng.uniform(-1, 1, (rows, n))
+    out = np.empty((rows, n))
+    kind = "reference"
+    if oracle.ref_available():
+        L = oracle.ref_cpu()
+        dp = C.POINTER(C.c_double)
+        L.ref_cpu_set_b.argtypes = [C.c_int, C.c_int, dp]
+        L.ref_cpu_rows.argtypes = [C.c_int, C.c_int, dp, dp]
+        L.ref_cpu_set_b(n, n, B.ctypes.data_as(dp))
+
+        def work(t):
+            a = np.ascontiguousarray(A[t * rows_per_thread:(t + 1) * rows_per_thread])
+            o = np.empty((rows_per_thread, n))
+            L.ref_cpu_rows(rows_per_thread, n, a.ctypes.data_as(dp), o.ctypes.data_as(dp))
+            out[t * rows_per_thread:(t + 1) * rows_per_thread] = o
+    else:
+        kind = "port"
+
+        def work(t):
+            sl = slice(t * rows_per_thread, (t + 1) * rows_per_thread)
+            out[sl] = oracle.gemm(A[sl], B, threads=1)
+
+    def step():
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(work, range(threads)))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    tflops = 2.0 * rows * n * n / dt / 1e12
+    sample = ("Matrix<double>::operator* (Kernel/cuda/src/Matrix.h:183-201) on %d rows x %d x %d per step "
+              "(%d threads x %d rows)" % (rows, n, n, threads, rows_per_thread))
+    line = {"impl": "reference", "metric": METRIC, "value": tflops, "unit": "TFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "reference CPU product, sample of the %d^3 GEMM" % n, "m": n, "n": n, "k": n},
+            "cpu_baseline": {"value": tflops, "unit": "TFLOP/s", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": tflops, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# -------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=8192)
+    ap.add_argument("--ref-rows", type=int, default=32)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / error leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+
+    import cucosma_b200 as cc
+
+    world, rank, local = dist_setup(args.gpus)
+    n = args.size
+    pk = peaks()
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    sms = props.multi_processor_count
+
+    A32 = make_inputs(n, 1 + 10 * rank, torch.float32)
+    B32 = make_inputs(n, 2 + 10 * rank, torch.float32)
+    C32 = torch.zeros((n, n), dtype=torch.float32, device="cuda")
+    A64 = make_inputs(n, 3 + 10 * rank, torch.float64)
+    B64 = make_inputs(n, 4 + 10 * rank, torch.float64)
+    C64 = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+
+    paths = [("bf16x3", A32, B32, C32, 0), ("native_f32", A32, B32, C32, 0), ("ozaki", A64, B64, C64, OZAKI_SLICES),
+             ("native_f64", A64, B64, C64, 0)]
+    flop = 2.0 * n * n * n
+    results, outs = {}, {}
+    clocks = None
+    for name, A, B, Cm, slices in paths:
+        prec = "native" if name.startswith("native") else name
+        d = cc.make_desc(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices)
+        try:
+            ws = cc.alloc_workspace(d)
+            cc.gemm(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices, workspace=ws)
+        except cc.CucosmaError as e:
+            if e.status == cc.NOT_SUPPORTED:
+                results[name] = {"available": False}
+                continue
+            raise
+        sampler = ClockSampler(local) if name == "bf16x3" or (clocks is None and name == "native_f32") else None
+        if sampler:
+            sampler.start()
+        ms, kern_ms, launches = time_path(cc, A, B, Cm, prec, slices, args.steps, args.warmup, world, ws)
+        if sampler:
+            c = sampler.stop()
+            if name == "bf16x3" or clocks is None:
+                clocks = c
+        ms = max_over_ranks(ms, world)
+        tf = flop / (ms * 1e-3) / 1e12
+        if name == "native_f32":
+            peak, peak_name = sms * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12, "FP32 SIMT (SMs x 128 x 2 x max clock)"
+        elif name == "native_f64":
+            peak, peak_name = sms * 64 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12, "FP64 (SMs x 64 x 2 x max clock)"
+        elif name == "bf16x3":
+            peak, peak_name = pk["bf16"] / 3, "measured bf16 dense / 3 products"
+        else:
+            peak = 2 * pk["bf16"] / (slices * (slices + 1) / 2)
+            peak_name = "INT8 dense (2 x measured bf16) / %d slice products" % (slices * (slices + 1) // 2)
+        results[name] = {"available": True, "ms": ms, "tflops": tf, "pct_of_peak": 100.0 * tf / peak,
+                         "peak_tflops": peak, "peak": peak_name, "kernel_ms": kern_ms, "launches_per_step":
+                         launches / args.steps, "workspace_bytes": (ws.numel() if ws is not None else 0)}
+        outs[name] = Cm.cpu().numpy().copy() if rank == 0 and not args.no_cpu else None
+
+    head = "bf16x3" if results.get("bf16x3", {}).get("available") else "native_f32"
+    hr = results[head]
+    A_h = A32.cpu().pin_memory()
+    B_h = B32.cpu().pin_memory()
+    C_h = torch.empty((n, n), dtype=torch.float32).pin_memory()
+    d = cc.make_desc(A32, B32, C32, precision=("bf16x3" if head == "bf16x3" else "native"))
+    ws = cc.alloc_workspace(d)
+    e2e_ms = e2e_path(cc, A_h, B_h, C_h, A32, B32, C32, "bf16x3" if head == "bf16x3" else "native", 0,
+                      max(3, args.steps // 2), 2, ws)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+
+    cpu, errs = (None, {})
+    if rank == 0 and not args.no_cpu:
+        cpu, errs = cpu_sample(n, A32.cpu().numpy(), B32.cpu().numpy(), A64.cpu().numpy(), B64.cpu().numpy(), outs)
+        for name, e in errs.items():
+            results[name]["error_vs_fp64"] = e
+
+    # roofline of the headline's main kernel (useful flops / kernel time)
+    kern_ms = hr.get("kernel_ms") or hr["ms"]
+    achieved = flop / (kern_ms * 1e-3) / 1e12
+    roof = {"bound": "tensor" if head == "bf16x3" else "fp32-simt", "achieved": achieved, "peak": hr["peak_tflops"],
+            "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"], "traffic": None,
+            "peak_source": pk["source"] + ": " + hr["peak"], "kernel_ms": kern_ms}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": hr["tflops"] * world, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3->f32" if head == "bf16x3" else "f32", "data": "synthetic",
+            "config": {"workload": "SGEMM %s %d^3, alpha=1 beta=0, U[-1,1]" % (head, n), "m": n, "n": n, "k": n,
+                       "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (%d MB per FP32 operand), no flush" % (n * n * 4 >> 20)},
+            "e2e": {"value": flop / (e2e_ms * 1e-3) / 1e12 * world, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": 2 * n * n * 4, "d2h_bytes_per_step": n * n * 4},
+            "gpu_launches": int(hr["launches_per_step"] * args.steps),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "results": results,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

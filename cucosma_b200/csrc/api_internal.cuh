@@ -1,0 +1,54 @@
+// api_internal.cuh -- host-side declarations shared by the C ABI translation units.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "../../include/cucosma.h"
+
+namespace cucosma {
+
+struct DeviceInfo {
+  bool valid = false;
+  int sms = 0, cc_major = 0, cc_minor = 0, l2_bytes = 0, smem_optin = 0;
+  int* status = nullptr;  // device address of the status word on this device
+};
+const DeviceInfo* device_info();
+struct WaitCtl;
+// Wait control for launches on the current device.
+void wait_ctl(const DeviceInfo* di, int** status, unsigned long long* timeout_ns);
+
+struct NativePlan {
+  int tiles_m, tiles_n, splits, swizzle;
+  int64_t kchunk, ldw;
+  size_t ws_bytes;
+};
+NativePlan plan_native(const cucosma_gemm_desc* d, int sms);
+
+cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B, const void* C);
+cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,
+                    cudaStream_t st);
+
+bool encode_2d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const void* base, uint64_t inner,
+               uint64_t outer, uint64_t row_stride_elems, uint32_t box_inner, uint32_t box_outer,
+               CUtensorMapSwizzle swz);
+bool encode_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const void* base, uint64_t d0, uint64_t d1,
+               uint64_t d2, uint64_t stride1_elems, uint64_t stride2_elems, uint32_t b0, uint32_t b1, uint32_t b2,
+               CUtensorMapSwizzle swz);
+
+// Tensor-core paths (BF16x3 / BF16x6 / Ozaki), tc_gemm.cu.
+cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const DeviceInfo* di);
+cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
+                       const DeviceInfo* di, cudaStream_t st);
+
+void* managed_workspace(size_t bytes);
+
+// Launch accounting and optional timing of the main GEMM kernel of each call:
+// note_launches() counts every kernel the library enqueues; prof_begin /
+// prof_end bracket the main kernel with CUDA events while profiling is on.
+void note_launches(int n);
+void prof_begin(cudaStream_t st);
+void prof_end(cudaStream_t st);
+
+}  // namespace cucosma

@@ -1,0 +1,53 @@
+// common.cuh -- shared device helpers: epilogue functors and the output
+// stage that applies C = epi(alpha*acc + beta*C).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ptx.cuh"
+
+namespace cucosma {
+
+enum Epilogue : int { kEpiNone = 0, kEpiSigmoid = 1, kEpiRelu = 2 };
+
+// Fused activation applied to the final value (cuCOSMAV100.cuh:2466-2476
+// holds the reference's ReLU / Sigmoid loops; sigmoid4.cuh:19-22 the formula).
+__device__ __forceinline__ float apply_epi(float v, int epi) {
+  if (epi == kEpiSigmoid) return 1.0f / (1.0f + expf(-v));
+  if (epi == kEpiRelu) return fmaxf(v, 0.0f);
+  return v;
+}
+__device__ __forceinline__ double apply_epi(double v, int epi) {
+  if (epi == kEpiSigmoid) return 1.0 / (1.0 + exp(-v));
+  if (epi == kEpiRelu) return fmax(v, 0.0);
+  return v;
+}
+
+// alpha/beta combination.  The reference scales the accumulator by ALPHA
+// first and then adds BETA*C (cuCOSMAV100.cuh:1582-1593, :901); written here
+// as one explicit FMA so every path (and the oracle) rounds the same way.
+// C is not read when beta == 0.
+template <typename T>
+__device__ __forceinline__ T combine(T acc, T alpha, T beta, const T* cptr) {
+  T v = alpha * acc;
+  if (beta != T(0)) v = fma(beta, *cptr, v);
+  return v;
+}
+
+template <typename T>
+struct Vec;
+template <>
+struct Vec<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
+__host__ __device__ constexpr int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ constexpr int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+}  // namespace cucosma

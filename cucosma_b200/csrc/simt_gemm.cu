@@ -1,0 +1,318 @@
+// simt_gemm.cu -- native FP32 (FFMA) and FP64 (DFMA) GEMM for sm_100a.
+//
+// Replaces the reference kernel cosmaSgemm_kernel (cuCOSMAV100.cuh:2505-2756)
+// and its split-K reduction (cosmaSplitKReduce.cuh:20-58) with a B200 design:
+//   * a producer warp streams A and B tiles with TMA into a 4-stage shared
+//     memory ring guarded by mbarriers (the reference double-buffers with
+//     __syncthreads and register-staged loads that transpose A on the way);
+//   * A tiles land row-major with the 64-byte TMA swizzle, so the compute
+//     warps read 8 rows x VEC k-values per LDS.128 without bank conflicts and
+//     no transposition is needed;
+//   * 8 compute warps hold a 128x128 CTA tile, 8x8 outputs per thread, rows
+//     interleaved by 4 within a warp's 32 rows;
+//   * split-K writes raw partial tiles to a caller-provided workspace and a
+//     separate kernel reduces them in ascending split order (deterministic),
+//     then applies alpha/beta and the epilogue, like cosmaSplitKReduce;
+//   * the block-index swizzle follows the reference's remap
+//     (cuCOSMAV100.cuh:2586-2603).
+#include "simt_gemm.cuh"
+
+namespace cucosma {
+
+template <typename T>
+__global__ void __launch_bounds__(simt::kThreads, 1)
+    simt_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     const SimtParams p) {
+  using namespace simt;
+  constexpr int BK = Cfg<T>::BK;
+  constexpr int VEC = Vec<T>::n;
+  using V = typename Vec<T>::type;
+  constexpr int A_STAGE = BM * BK * (int)sizeof(T);
+  constexpr int B_STAGE = BK * BN * (int)sizeof(T);
+  constexpr int KG = BK / VEC;  // k-groups per stage (one LDS.128 of A covers VEC k)
+  static_assert(KG == 4, "stage holds four 16-byte chunks per A row");
+  static_assert(BK * sizeof(T) == 64, "A rows are 64 bytes (64-byte swizzle span)");
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* As = smem;
+  uint8_t* Bs = smem + STAGES * A_STAGE;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * (A_STAGE + B_STAGE));
+  uint64_t* empty = full + STAGES;
+
+  // Block-index remap (reference semantics, cuCOSMAV100.cuh:2586-2603).
+  int tile_n, tile_m;
+  if (p.swizzle > 1) {
+    tile_n = blockIdx.x / p.swizzle;
+    tile_m = blockIdx.y * p.swizzle + blockIdx.x % p.swizzle;
+    if (tile_m >= p.tiles_m) return;
+  } else {
+    tile_n = blockIdx.x;
+    tile_m = blockIdx.y;
+  }
+  const int m0 = tile_m * BM, n0 = tile_n * BN;
+  const int64_t kbeg = (int64_t)blockIdx.z * p.kchunk;
+  const int64_t kend = min((int64_t)p.k, kbeg + p.kchunk);
+  const int nkb = kend > kbeg ? (int)ceil_div(kend - kbeg, BK) : 0;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kComputeWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Producer role (thread 0): load k-block kb into stage kb % STAGES once all
+  // warps released that stage.  Returns false if the wait for it expired.
+  int issued = 0;
+  auto produce = [&](int kb) -> bool {
+    const int s = kb % STAGES;
+    const uint32_t ph = (kb / STAGES) & 1;
+    if (!mbar_wait(&empty[s], ph ^ 1, kErrTimeoutEmpty, p.ctl)) return false;
+    mbar_arrive_expect_tx(&full[s], A_STAGE + B_STAGE);
+    const int kx = (int)(kbeg + (int64_t)kb * BK);
+    tma_load_2d(As + s * A_STAGE, &tmA, kx, m0, &full[s]);
+    tma_load_2d(Bs + s * B_STAGE, &tmB, n0, kx, &full[s]);
+    issued = kb + 1;
+    return true;
+  };
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+    for (int kb = 0; kb < min(nkb, STAGES - 1) && ok; ++kb) ok = produce(kb);
+  }
+
+  // ---------------------------------------------------------------- compute
+  const int wm = warp >> 1, wn = warp & 1;  // 4 x 2 warps, warp tile 32 x 64
+  const int tx = lane & 7, ty = lane >> 3;  // 8 x 4 threads
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+
+  // Byte offsets (within a stage) of this thread's A rows (swizzle applied
+  // per chunk) and B columns.
+  int a_row_off[8], a_sw[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = wm * 32 + ty + 4 * i;
+    a_row_off[i] = r * 64;
+    a_sw[i] = (r >> 1) & 3;
+  }
+  constexpr int NJ = 8 / VEC;  // vectors per thread along N
+  const int b_col = wn * 64 + tx * VEC;
+
+  for (int kb = 0; kb < nkb && ok; ++kb) {
+    if (threadIdx.x == 0 && kb + STAGES - 1 < nkb) ok = produce(kb + STAGES - 1);
+    const int s = kb % STAGES;
+    if (!mbar_wait(&full[s], (kb / STAGES) & 1, kErrTimeoutFull, p.ctl)) {
+      ok = false;
+      break;
+    }
+    const uint8_t* as = As + s * A_STAGE;
+    const T* bs = reinterpret_cast<const T*>(Bs + s * B_STAGE);
+#pragma unroll
+    for (int kg = 0; kg < KG; ++kg) {
+      T a[8][VEC];
+      T b[VEC][8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const V v = *reinterpret_cast<const V*>(as + a_row_off[i] + ((kg ^ a_sw[i]) << 4));
+        const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) a[i][e] = pv[e];
+      }
+#pragma unroll
+      for (int kk = 0; kk < VEC; ++kk) {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const V v = *reinterpret_cast<const V*>(bs + (kg * VEC + kk) * BN + b_col + j * 8 * VEC);
+          const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) b[kk][j * VEC + e] = pv[e];
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < VEC; ++kk)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i][kk], b[kk][j], acc[i][j]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok) {
+    // A wait expired.  Thread 0 drains (bounded) every load it issued that
+    // may still be in flight, so no copy targets this CTA after it exits.
+    if (threadIdx.x == 0)
+      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
+        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, kErrTimeoutDrain, p.ctl);
+    return;
+  }
+
+  // --------------------------------------------------------------- epilogue
+  const T alpha = (T)p.alpha, beta = (T)p.beta;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = m0 + wm * 32 + ty + 4 * i;
+    if (r >= p.m) continue;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int c = n0 + b_col + j * 8 * VEC;
+      if (c >= p.n) continue;
+      if (p.partial) {
+        T* w = reinterpret_cast<T*>(p.out) + (int64_t)blockIdx.z * p.ws_split_stride + (int64_t)r * p.ldo + c;
+        if (c + VEC <= p.n) {
+          V v;
+          T* pv = reinterpret_cast<T*>(&v);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) pv[e] = acc[i][j * VEC + e];
+          *reinterpret_cast<V*>(w) = v;
+        } else {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e)
+            if (c + e < p.n) w[e] = acc[i][j * VEC + e];
+        }
+      } else {
+        T* o = reinterpret_cast<T*>(p.out) + (int64_t)r * p.ldo + c;
+        if (c + VEC <= p.n) {
+          V cv;
+          if (beta != T(0)) cv = *reinterpret_cast<const V*>(o);
+          const T* pc = reinterpret_cast<const T*>(&cv);
+          V v;
+          T* pv = reinterpret_cast<T*>(&v);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) pv[e] = apply_epi(combine(acc[i][j * VEC + e], alpha, beta, pc + e), p.epilogue);
+          *reinterpret_cast<V*>(o) = v;
+        } else {
+#pragma unroll
+          for (int e = 0; e < VEC; ++e)
+            if (c + e < p.n) o[e] = apply_epi(combine(acc[i][j * VEC + e], alpha, beta, o + e), p.epilogue);
+        }
+      }
+    }
+  }
+}
+
+// Deterministic split-K reduction: C = epi(alpha * sum_z ws[z] + beta*C),
+// z ascending, the sum accumulated in T (cosmaSplitKReduce.cuh:31-40).
+template <typename T>
+__global__ void splitk_reduce_kernel(const T* __restrict__ ws, int64_t split_stride, int64_t ldw, int splits, T* C,
+                                     int64_t ldc, int m, int n, double alpha_d, double beta_d, int epi) {
+  constexpr int VEC = Vec<T>::n;
+  using V = typename Vec<T>::type;
+  const T alpha = (T)alpha_d, beta = (T)beta_d;
+  const int64_t nv = ceil_div(n, VEC);
+  const int64_t total = (int64_t)m * nv;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / nv;
+    const int c = (int)(idx - r * nv) * VEC;
+    const T* w = ws + r * ldw + c;
+    T* o = C + r * ldc + c;
+    if (c + VEC <= n) {
+      V s = *reinterpret_cast<const V*>(w);
+      T* ps = reinterpret_cast<T*>(&s);
+      for (int z = 1; z < splits; ++z) {
+        const V t = *reinterpret_cast<const V*>(w + z * split_stride);
+        const T* pt = reinterpret_cast<const T*>(&t);
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) ps[e] += pt[e];
+      }
+      V cv;
+      if (beta != T(0)) cv = *reinterpret_cast<const V*>(o);
+      const T* pc = reinterpret_cast<const T*>(&cv);
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) ps[e] = apply_epi(combine(ps[e], alpha, beta, pc + e), epi);
+      *reinterpret_cast<V*>(o) = s;
+    } else {
+      for (int e = 0; c + e < n; ++e) {
+        T s = w[e];
+        for (int z = 1; z < splits; ++z) s += w[z * split_stride + e];
+        o[e] = apply_epi(combine(s, alpha, beta, o + e), epi);
+      }
+    }
+  }
+}
+
+// C = epi(beta*C) on an m x n region (alpha == 0 or k == 0: no product term).
+template <typename T>
+__global__ void scale_kernel(T* C, int64_t ldc, int m, int n, double beta_d, int epi) {
+  const T beta = (T)beta_d;
+  const int64_t total = (int64_t)m * n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / n, c = idx - r * n;
+    T* o = C + r * ldc + c;
+    const T v = beta != T(0) ? beta * *o : T(0);
+    *o = apply_epi(v, epi);
+  }
+}
+
+// ------------------------------------------------------------------- launch
+namespace simt {
+
+template <typename T>
+size_t smem_bytes() {
+  constexpr int BK = Cfg<T>::BK;
+  return 1024 + STAGES * (BM * BK + BK * BN) * sizeof(T) + 2 * STAGES * sizeof(uint64_t);
+}
+
+template <typename T>
+cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, cudaStream_t stream) {
+  static bool attr_set = false;  // per process; the attribute is per function
+  const size_t smem = smem_bytes<T>();
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(simt_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dim3 grid;
+  if (p.swizzle > 1) {
+    grid = dim3(p.tiles_n * p.swizzle, (unsigned)ceil_div(p.tiles_m, p.swizzle), p.splits);
+  } else {
+    grid = dim3(p.tiles_n, p.tiles_m, p.splits);
+  }
+  simt_gemm_kernel<T><<<grid, kThreads, smem, stream>>>(tmA, tmB, p);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_reduce(const T* ws, int64_t split_stride, int64_t ldw, int splits, T* C, int64_t ldc, int m, int n,
+                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream) {
+  const int64_t work = (int64_t)m * ceil_div(n, Vec<T>::n);
+  const int threads = 256;
+  int64_t blocks = ceil_div(work, threads);
+  blocks = std::min<int64_t>(blocks, (int64_t)num_sms * 8);
+  if (blocks < 1) blocks = 1;
+  splitk_reduce_kernel<T><<<(unsigned)blocks, threads, 0, stream>>>(ws, split_stride, ldw, splits, C, ldc, m, n, alpha,
+                                                                    beta, epi);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, int num_sms, cudaStream_t stream) {
+  const int64_t work = (int64_t)m * n;
+  int64_t blocks = std::min<int64_t>(ceil_div(work, 256), (int64_t)num_sms * 8);
+  if (blocks < 1) blocks = 1;
+  scale_kernel<T><<<(unsigned)blocks, 256, 0, stream>>>(C, ldc, m, n, beta, epi);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_gemm<float>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
+template cudaError_t launch_gemm<double>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
+template cudaError_t launch_reduce<float>(const float*, int64_t, int64_t, int, float*, int64_t, int, int, double, double,
+                                          int, int, cudaStream_t);
+template cudaError_t launch_reduce<double>(const double*, int64_t, int64_t, int, double*, int64_t, int, int, double,
+                                           double, int, int, cudaStream_t);
+template cudaError_t launch_scale<float>(float*, int64_t, int, int, double, int, int, cudaStream_t);
+template cudaError_t launch_scale<double>(double*, int64_t, int, int, double, int, int, cudaStream_t);
+template size_t smem_bytes<float>();
+template size_t smem_bytes<double>();
+
+}  // namespace simt
+}  // namespace cucosma

@@ -1,0 +1,57 @@
+// simt_gemm.cuh -- parameters and launchers of the native FP32/FP64 kernels.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace cucosma {
+
+struct SimtParams {
+  int m, n, k;
+  int kchunk;    // K extent of one split (multiple of the stage depth BK)
+  int splits;    // grid.z
+  int swizzle;   // block-index remap width (1 = none)
+  int tiles_m, tiles_n;
+  int partial;   // 1: write raw partial sums to out[z] (split-K workspace)
+  int epilogue;
+  double alpha, beta;
+  void* out;              // C, or the split-K workspace
+  int64_t ldo;            // row stride of out (elements)
+  int64_t ws_split_stride;  // elements between consecutive splits in the workspace
+  WaitCtl ctl;
+};
+
+namespace simt {
+constexpr int BM = 128, BN = 128, STAGES = 4;
+// Eight warps, all computing; thread 0 also issues the TMA loads.  (A ninth,
+// producer-only warp would put three warps in one register-file quadrant
+// and cap every thread at 168 registers, which the FP64 8x8 tile exceeds.)
+constexpr int kComputeWarps = 8;
+constexpr int kThreads = kComputeWarps * 32;
+
+template <typename T>
+struct Cfg;
+template <>
+struct Cfg<float> {
+  static constexpr int BK = 16;  // 64-byte A rows
+};
+template <>
+struct Cfg<double> {
+  static constexpr int BK = 8;
+};
+
+template <typename T>
+size_t smem_bytes();
+template <typename T>
+cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_reduce(const T* ws, int64_t split_stride, int64_t ldw, int splits, T* C, int64_t ldc, int m, int n,
+                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, int num_sms, cudaStream_t stream);
+}  // namespace simt
+
+}  // namespace cucosma

@@ -1,0 +1,133 @@
+/*
+ * cucosma.h -- C ABI of the cuCOSMA-compatible GEMM library for NVIDIA B200 (sm_100a).
+ *
+ * Computes C = epi(alpha * A*B + beta * C) on row-major matrices in device
+ * memory: A is m x k (row stride lda), B is k x n (ldb), C is m x n (ldc),
+ * strides in elements.  This replaces the reference's kernel API
+ *     cublasStatus_t cosmaSgemm(const TYPE* A, int lda, const TYPE* B, int ldb,
+ *                               TYPE* C, int ldc)          (Kernel/cuda/src/cuCOSMAV100.cuh:2774-2776)
+ * whose M, N, K, ALPHA, BETA, TYPE and tiling were compile-time macros
+ * (Kernel/cuda/src/config.h:9-31).  Here they are fields of a descriptor (or
+ * arguments), tiling and split-K are chosen by the library (or its tuner),
+ * and the compile-time template form lives in cucosma.hpp.
+ *
+ * Plain C: pointers, sizes and integers only.  No entry point throws or
+ * exits; all return a cucosma_status.  All GPU work is enqueued on the
+ * caller's stream (a cudaStream_t passed as void*; NULL = legacy default).
+ *
+ * Alignment: A, B and C must be 16-byte aligned and every row must start on
+ * a 16-byte boundary (lda, ldb, ldc * sizeof(element) multiples of 16), the
+ * reference's "aligned rows" contract (cudaMallocPitch pitches,
+ * Kernel/cuda/src/test_correctness.h:55-58).  Otherwise the call returns
+ * CUCOSMA_STATUS_MISALIGNED and launches nothing.
+ */
+#ifndef CUCOSMA_H_
+#define CUCOSMA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUCOSMA_VERSION 100 /* 0.1.0 */
+
+#if defined(__GNUC__)
+#define CUCOSMA_API __attribute__((visibility("default")))
+#else
+#define CUCOSMA_API
+#endif
+
+typedef enum cucosma_status {
+  CUCOSMA_STATUS_SUCCESS = 0,
+  CUCOSMA_STATUS_INVALID_VALUE = 1,       /* bad size, stride, null pointer or enum */
+  CUCOSMA_STATUS_MISALIGNED = 2,          /* pointer or row stride not 16-byte aligned */
+  CUCOSMA_STATUS_NOT_SUPPORTED = 3,       /* combination not implemented (e.g. BF16X3 on FP64) */
+  CUCOSMA_STATUS_WORKSPACE_TOO_SMALL = 4, /* workspace_bytes below cucosma_gemm_workspace_size */
+  CUCOSMA_STATUS_LAUNCH_FAILED = 5,       /* a CUDA launch or API call failed */
+  CUCOSMA_STATUS_TIMEOUT = 6,             /* a device-side bounded wait expired (see cucosma_device_status) */
+  CUCOSMA_STATUS_ARCH_MISMATCH = 7,       /* current device is not sm_100 */
+  CUCOSMA_STATUS_ALLOC_FAILED = 8,        /* library-managed workspace could not be allocated */
+  CUCOSMA_STATUS_INTERNAL_ERROR = 9
+} cucosma_status;
+
+typedef enum cucosma_dtype { CUCOSMA_R_32F = 0, CUCOSMA_R_64F = 1 } cucosma_dtype;
+
+typedef enum cucosma_precision {
+  CUCOSMA_PRECISION_NATIVE = 0, /* FFMA (FP32) / DFMA (FP64) SIMT kernels */
+  CUCOSMA_PRECISION_BF16X3 = 1, /* FP32: hi/lo BF16 split, 3 tensor-core products, FP32 accumulation */
+  CUCOSMA_PRECISION_BF16X6 = 2, /* FP32: hi/mid/lo BF16 split, 6 tensor-core products */
+  CUCOSMA_PRECISION_OZAKI = 3   /* FP64: INT8 slices, exact INT32 products, FP64 recombination */
+} cucosma_precision;
+
+typedef enum cucosma_epilogue {
+  CUCOSMA_EPILOGUE_NONE = 0,
+  CUCOSMA_EPILOGUE_SIGMOID = 1, /* 1/(1+exp(-x)) of the final value (cuCOSMAV100.cuh:2472-2476) */
+  CUCOSMA_EPILOGUE_RELU = 2     /* max(x, 0) (cuCOSMAV100.cuh:2466-2470) */
+} cucosma_epilogue;
+
+typedef struct cucosma_gemm_desc {
+  int64_t m, n, k;        /* M, N, K of config.h */
+  int64_t lda, ldb, ldc;  /* row strides in elements */
+  int32_t dtype;          /* cucosma_dtype (TYPE of config.h) */
+  int32_t precision;      /* cucosma_precision */
+  int32_t slices;         /* Ozaki slice count 4..12, 0 = default (8) */
+  int32_t epilogue;       /* cucosma_epilogue */
+  double alpha, beta;     /* ALPHA, BETA of config.h; C is not read when beta == 0 */
+  int32_t split_k;        /* SPLIT_K: 0 = library/tuner choice, >= 1 forced */
+  int32_t swizzle;        /* SWIZZLE: 0 = library choice, >= 1 forced block-index remap width */
+  int32_t tile;           /* 0 = library/tuner choice, else a kernel configuration id */
+  int32_t flags;          /* reserved, must be 0 */
+} cucosma_gemm_desc;
+
+/* Fill *d with defaults: FP32, native, alpha = 1, beta = 0, no epilogue, auto split-K. */
+CUCOSMA_API void cucosma_gemm_desc_init(cucosma_gemm_desc* d);
+
+/* Bytes of device workspace cucosma_gemm needs for *d (0 when none). */
+CUCOSMA_API cucosma_status cucosma_gemm_workspace_size(const cucosma_gemm_desc* d, size_t* bytes);
+
+/* C = epi(alpha*A*B + beta*C).  workspace may be NULL when the size is 0.
+ * Allocation-free; asynchronous on stream.  Replaces cosmaSgemm
+ * (cuCOSMAV100.cuh:2774-2848) including its split-K workspace path
+ * (:2824-2838, which allocated and freed the workspace on every call). */
+CUCOSMA_API cucosma_status cucosma_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/* Reference-shaped FP32 / FP64 entry points: the compile-time M, N, K, ALPHA,
+ * BETA of config.h become arguments (cuCOSMAV100.cuh:2774; the FP64 form is
+ * the TYPE=double instantiation).  Native arithmetic, no epilogue; any split-K
+ * workspace is library-managed (allocated once per device and grown on
+ * demand, like the reference's internal cudaMalloc but not per call). */
+CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
+                             float beta, float* C, int ldc, void* stream);
+CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
+                             double beta, double* C, int ldc, void* stream);
+
+/* Synchronises the device, then returns and clears the device status word:
+ * CUCOSMA_STATUS_TIMEOUT if any kernel gave up on a bounded wait since the
+ * last call, CUCOSMA_STATUS_LAUNCH_FAILED on a CUDA error, else SUCCESS.
+ * *detail (optional) receives the raw device code. */
+CUCOSMA_API cucosma_status cucosma_device_status(int* detail);
+
+/* Limit for every device-side wait (default 4 s).  Applies to later launches. */
+CUCOSMA_API cucosma_status cucosma_set_wait_timeout_ns(uint64_t ns);
+
+CUCOSMA_API const char* cucosma_get_error_string(cucosma_status s);
+CUCOSMA_API int cucosma_get_version(void);
+
+/* Observability (no counterpart in the reference, which timed its kernel with
+ * nvprof, Kernel/cuda/run.sh:291).
+ * cucosma_launch_count: kernels this library has enqueued in this process.
+ * cucosma_profile_start / _stop: while on, every call records CUDA events on
+ * its stream around its main GEMM kernel; _stop synchronises those events and
+ * returns the summed kernel time (ms) and the number of timed launches. */
+CUCOSMA_API unsigned long long cucosma_launch_count(void);
+CUCOSMA_API cucosma_status cucosma_profile_start(void);
+CUCOSMA_API cucosma_status cucosma_profile_stop(double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUCOSMA_H_ */

@@ -1,0 +1,179 @@
+"""GPU parity tests of the native FP32 (FFMA) / FP64 (DFMA) path through the
+C ABI, against the FP64 oracle (rigorous componentwise bound), the golden
+fixtures, and the reference kernel cosmaSgemm built from its own sources
+(oracle/_ref, when present)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import cucosma_b200 as cc
+import oracle
+from tests._util import check_against_oracle, to_dev, uniform
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(1, 1, 1), (7, 5, 3), (4, 8, 300), (127, 127, 127), (128, 128, 128), (129, 257, 65), (300, 200, 100),
+          (1000, 4, 17), (33, 1000, 5), (512, 384, 1024)]
+
+
+def run(A, B, Cin, alpha, beta, dtype, epilogue="none", ld_pad=0, **kw):
+    import torch
+
+    es = np.dtype(dtype).itemsize
+    pad = ld_pad * (16 // es)
+    dA = to_dev(A.astype(dtype), ld=None if not pad else A.shape[1] + pad + (-(A.shape[1]) % (16 // es)))
+    dB = to_dev(B.astype(dtype), ld=None if not pad else B.shape[1] + pad + (-(B.shape[1]) % (16 // es)))
+    dC = to_dev(Cin.astype(dtype))
+    cc.gemm(dA, dB, dC, alpha, beta, epilogue=epilogue, **kw)
+    torch.cuda.synchronize()
+    return dC.cpu().numpy()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d" % s for s in SHAPES])
+def test_native_vs_oracle(cuda, shape, dtype):
+    m, n, k = shape
+    A = uniform(1, (m, k), dtype)
+    B = uniform(2, (k, n), dtype)
+    Cin = uniform(3, (m, n), dtype)
+    out = run(A, B, Cin, 1.0, 0.5, dtype)
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.5, 0.0), (0.75, 1.0), (2.0, -0.5), (0.0, 0.5), (0.0, 0.0)])
+def test_alpha_beta(cuda, dtype, alpha, beta):
+    A = uniform(4, (200, 150), dtype)
+    B = uniform(5, (150, 170), dtype)
+    Cin = uniform(6, (200, 170), dtype)
+    out = run(A, B, Cin, alpha, beta, dtype)
+    check_against_oracle(out, A, B, Cin, alpha, beta, oracle.EPI_NONE, dtype)
+
+
+def test_beta_zero_ignores_nan_c(cuda):
+    A = uniform(7, (64, 64))
+    B = uniform(8, (64, 64))
+    Cin = np.full((64, 64), np.nan, np.float32)
+    out = run(A, B, Cin, 1.0, 0.0, np.float32)
+    assert np.isfinite(out).all()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("epi", ["sigmoid", "relu"])
+def test_fused_epilogue(cuda, dtype, epi):
+    A = uniform(9, (257, 130), dtype)
+    B = uniform(10, (130, 300), dtype)
+    Cin = uniform(11, (257, 300), dtype)
+    out = run(A, B, Cin, 1.0, 0.5, dtype, epilogue=epi)
+    code = oracle.EPI_SIGMOID if epi == "sigmoid" else oracle.EPI_RELU
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, code, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("split_k", [1, 2, 3, 7, 40])
+def test_split_k(cuda, dtype, split_k):
+    A = uniform(12, (130, 2000), dtype)
+    B = uniform(13, (2000, 129), dtype)
+    Cin = uniform(14, (130, 129), dtype)
+    out = run(A, B, Cin, 1.0, 0.5, dtype, split_k=split_k)
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, dtype)
+
+
+def test_split_k_sigmoid(cuda):
+    A = uniform(15, (100, 3000))
+    B = uniform(16, (3000, 90))
+    Cin = uniform(17, (100, 90))
+    out = run(A, B, Cin, 0.5, 0.5, np.float32, epilogue="sigmoid", split_k=5)
+    check_against_oracle(out, A, B, Cin, 0.5, 0.5, oracle.EPI_SIGMOID, np.float32)
+
+
+@pytest.mark.parametrize("swizzle", [2, 3, 4, 8])
+def test_swizzle(cuda, swizzle):
+    A = uniform(18, (1000, 64))
+    B = uniform(19, (64, 700))
+    Cin = uniform(20, (1000, 700))
+    out = run(A, B, Cin, 1.0, 0.5, np.float32, swizzle=swizzle)
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, np.float32)
+
+
+def test_padded_leading_dimensions(cuda):
+    A = uniform(21, (77, 93))
+    B = uniform(22, (93, 61))
+    Cin = uniform(23, (77, 61))
+    out = run(A, B, Cin, 1.0, 0.5, np.float32, ld_pad=3)
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, np.float32)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+def test_deterministic_bitwise(cuda, dtype):
+    A = uniform(24, (300, 5000), dtype)
+    B = uniform(25, (5000, 200), dtype)
+    Cin = uniform(26, (300, 200), dtype)
+    outs = [run(A, B, Cin, 1.0, 0.5, dtype, split_k=6) for _ in range(3)]
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "gemm_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_golden_fixtures(cuda, path):
+    g = np.load(path)
+    A, B = g["A"], g["B"]
+    Cin = np.zeros((A.shape[0], B.shape[1]), np.float32)
+    out = run(A, B, Cin, 1.0, 0.0, np.float32)
+    k = A.shape[1]
+    absab = oracle.gemm(np.abs(A), np.abs(B))
+    assert np.all(np.abs(out - g["prod_f64"]) <= (k + 2) * 2.0 ** -24 * absab + 1e-30)
+
+
+def test_reference_shaped_entry_point(cuda):
+    import torch
+
+    for dtype in (np.float32, np.float64):
+        A = uniform(27, (150, 80), dtype)
+        B = uniform(28, (80, 140), dtype)
+        Cin = uniform(29, (150, 140), dtype)
+        dA, dB, dC = to_dev(A), to_dev(B), to_dev(Cin)
+        cc.cosma_sgemm(dA, dB, dC, 1.0, 0.5)
+        torch.cuda.synchronize()
+        check_against_oracle(dC.cpu().numpy(), A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, dtype)
+
+
+def test_device_status_clean_after_runs(cuda):
+    s, code = cc.device_status()
+    assert s == cc.SUCCESS and code == 0
+
+
+# --------------------------------------------------------- reference kernel
+
+
+REF_TAGS = [t for t in oracle.ref_kernel_tags() if "8192" not in t]
+
+
+@pytest.mark.parametrize("tag", REF_TAGS)
+def test_parity_with_reference_kernel(cuda, tag):
+    """Same seeded inputs through the reference kernel (compiled unmodified for
+    sm_100a) and through this library: both inside the FP64-oracle bound."""
+    import torch
+
+    ref = oracle.RefKernel(tag)
+    c = ref.config
+    dtype = np.float32 if c["elem"] == 4 else np.float64
+    m, n, k = c["m"], c["n"], c["k"]
+    A = uniform(31, (m, k), dtype)
+    B = uniform(32, (k, n), dtype)
+    Cin = uniform(33, (m, n), dtype)
+    pitch = 512 // np.dtype(dtype).itemsize  # cudaMallocPitch-like rows
+    ld = lambda cols: -(-cols // pitch) * pitch  # noqa: E731
+    rA, rB, rC = to_dev(A, ld(k)), to_dev(B, ld(n)), to_dev(Cin, ld(n))
+    rc = ref(rA.data_ptr(), rA.stride(0), rB.data_ptr(), rB.stride(0), rC.data_ptr(), rC.stride(0))
+    torch.cuda.synchronize()
+    assert rc == 0
+    out_ref = rC.cpu().numpy()
+    out = run(A, B, Cin, ref.alpha, ref.beta, dtype)
+    e_ref = check_against_oracle(out_ref, A, B, Cin, ref.alpha, ref.beta, oracle.EPI_NONE, dtype)
+    e_own = check_against_oracle(out, A, B, Cin, ref.alpha, ref.beta, oracle.EPI_NONE, dtype)
+    print(tag, "reference", e_ref, "cucosma", e_own)
