@@ -46,13 +46,28 @@ class GemmDesc(C.Structure):
     ]
 
 
+class PlanInfo(C.Structure):
+    """Mirror of cucosma_plan_info (include/cucosma.h)."""
+
+    _fields_ = [
+        ("path", C.c_int32), ("tile_m", C.c_int32), ("tile_n", C.c_int32), ("tile_k", C.c_int32),
+        ("splits", C.c_int32), ("band", C.c_int32), ("slices", C.c_int32), ("launches", C.c_int32),
+        ("kchunk", C.c_int64), ("kpad", C.c_int64),
+        ("workspace_bytes", C.c_uint64), ("off_a", C.c_uint64), ("off_b", C.c_uint64), ("off_ea", C.c_uint64),
+        ("off_eb", C.c_uint64), ("off_part", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
 _lib = None
 
 # Every symbol include/cucosma.h declares; checked when the library loads.
 EXPORTS = [
     "cucosma_gemm_desc_init", "cucosma_gemm_workspace_size", "cucosma_gemm", "cucosma_sgemm", "cucosma_dgemm",
     "cucosma_device_status", "cucosma_set_wait_timeout_ns", "cucosma_get_error_string", "cucosma_get_version",
-    "cucosma_launch_count", "cucosma_profile_start", "cucosma_profile_stop",
+    "cucosma_launch_count", "cucosma_profile_start", "cucosma_profile_stop", "cucosma_gemm_get_plan",
 ]
 
 
@@ -78,6 +93,7 @@ def lib():
     L.cucosma_get_version.restype = C.c_int
     L.cucosma_launch_count.restype = C.c_ulonglong
     L.cucosma_profile_stop.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.cucosma_gemm_get_plan.argtypes = [C.POINTER(GemmDesc), C.POINTER(PlanInfo)]
     for name in EXPORTS:
         if name not in ("cucosma_gemm_desc_init", "cucosma_get_error_string", "cucosma_get_version",
                         "cucosma_launch_count"):
@@ -139,6 +155,12 @@ def make_desc(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none"
     d.alpha, d.beta = float(alpha), float(beta)
     d.split_k, d.swizzle, d.slices, d.tile = int(split_k), int(swizzle), int(slices), int(tile)
     return d
+
+
+def get_plan(desc):
+    info = PlanInfo()
+    check(lib().cucosma_gemm_get_plan(C.byref(desc), C.byref(info)), "cucosma_gemm_get_plan")
+    return info.as_dict()
 
 
 def workspace_size(desc):

@@ -331,6 +331,31 @@ extern "C" cucosma_status cucosma_gemm_workspace_size(const cucosma_gemm_desc* d
   return workspace_size(d, bytes, di);
 }
 
+extern "C" cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cucosma_plan_info* info) {
+  if (!d || !info) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (d->m < 0 || d->n < 0 || d->k < 0) return CUCOSMA_STATUS_INVALID_VALUE;
+  std::memset(info, 0, sizeof(*info));
+  const DeviceInfo* di = device_info();
+  if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  if (d->precision == CUCOSMA_PRECISION_NATIVE) {
+    const NativePlan pl = plan_native(d, di->sms);
+    info->path = 0;
+    info->tile_m = simt::BM;
+    info->tile_n = simt::BN;
+    info->tile_k = simt_bk(d->dtype);
+    info->splits = pl.splits;
+    info->band = pl.swizzle;
+    info->slices = 1;
+    info->launches = pl.splits > 1 ? 2 : 1;
+    info->kchunk = pl.kchunk;
+    info->kpad = d->k;
+    info->workspace_bytes = pl.ws_bytes;
+    return CUCOSMA_STATUS_SUCCESS;
+  }
+  tc_plan_info(d, di, info);
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
 extern "C" cucosma_status cucosma_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
                                        void* workspace, size_t workspace_bytes, void* stream) {
   return gemm(d, A, B, C, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));

@@ -39,6 +39,7 @@ bool encode_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const v
 
 // Tensor-core paths (BF16x3 / BF16x6 / Ozaki), tc_gemm.cu.
 cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const DeviceInfo* di);
+void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info);
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                        const DeviceInfo* di, cudaStream_t st);
 

@@ -1,0 +1,250 @@
+// split.cu -- operand pre-passes of the tensor-core precision paths.
+//
+// BF16 split (BF16x3 / BF16x6 SGEMM): every FP32 entry x becomes terms
+// t0 + t1 (+ t2) with t_i = RN_bf16(x - t0 - ... - t_{i-1}); each residual
+// subtraction is exact in FP32.  A (M x K, row-major) keeps its layout;
+// B (K x N, row-major) is written transposed (N x K) so that both operands
+// are K-major for the tensor cores.  Planes: [nterms][rows][kpad].
+//
+// Ozaki slicing (INT8 DGEMM): per row of A / per column of B the exponent
+// e with |x| < 2^e over the row / column; x * 2^-e is cut into s signed
+// 7-bit integer slices q_t = trunc(r * 2^7), r <- r * 2^7 - q_t, exact in
+// FP64.  A slices [s][M][kpad], B slices [s][N][kpad] (transposed).
+//
+// All pre-passes are HBM-bound elementwise / transpose kernels.
+#include <cuda_bf16.h>
+
+#include "split.cuh"
+
+namespace cucosma {
+
+// ------------------------------------------------------------------ BF16
+__device__ __forceinline__ void split_bf16_value(float x, int nterms, __nv_bfloat16 (&t)[3]) {
+  float r = x;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i < nterms) {
+      t[i] = __float2bfloat16_rn(r);
+      r = r - __bfloat162float(t[i]);
+    }
+  }
+}
+
+// A: rows x cols (ld elements) -> planes [nterms][rows][kpad], same layout.
+// Each thread converts 4 consecutive columns.
+__global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
+                                       int nterms, __nv_bfloat16* __restrict__ out) {
+  const int64_t c4 = ceil_div(cols, 4);
+  const int64_t total = (int64_t)rows * c4;
+  const int64_t plane = (int64_t)rows * kpad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / c4;
+    const int c = (int)(idx - r * c4) * 4;
+    const float* src = A + r * lda + c;
+    float v[4];
+    if (c + 4 <= cols) {
+      const float4 q = *reinterpret_cast<const float4*>(src);
+      v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[e] = c + e < cols ? src[e] : 0.f;
+    }
+    __nv_bfloat16 t[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) split_bf16_value(v[e], nterms, t[e]);
+    for (int i = 0; i < nterms; ++i) {
+      __nv_bfloat16* dst = out + i * plane + r * kpad + c;
+      if (c + 4 <= kpad) {
+        // kpad is a multiple of 8: an aligned 8-byte store
+        __nv_bfloat162 lo = __halves2bfloat162(t[0][i], t[1][i]);
+        __nv_bfloat162 hi = __halves2bfloat162(t[2][i], t[3][i]);
+        uint2 pk;
+        pk.x = *reinterpret_cast<uint32_t*>(&lo);
+        pk.y = *reinterpret_cast<uint32_t*>(&hi);
+        *reinterpret_cast<uint2*>(dst) = pk;
+      }
+    }
+  }
+}
+
+// B: K x N (ld elements) -> planes [nterms][N][kpad] (transposed), through a
+// 32 x 32 shared-memory tile.  Block = 32 x 8 threads.
+__global__ void split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
+                                       int nterms, __nv_bfloat16* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
+  const int64_t plane = (int64_t)ncols * kpad;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int k = k0 + i, n = n0 + threadIdx.x;
+    tile[i][threadIdx.x] = (k < krows && n < ncols) ? B[(int64_t)k * ldb + n] : 0.f;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int n = n0 + i, k = k0 + threadIdx.x;
+    if (n < ncols && k < kpad) {
+      __nv_bfloat16 t[3];
+      split_bf16_value(tile[threadIdx.x][i], nterms, t);
+      for (int j = 0; j < nterms; ++j) out[j * plane + (int64_t)n * kpad + k] = t[j];
+    }
+  }
+}
+
+// ----------------------------------------------------------------- Ozaki
+// frexp-style exponent of the largest magnitude: |x| < 2^e for all x.
+__device__ __forceinline__ int exp_of(double amax) {
+  if (amax == 0.0) return 0;
+  int e;
+  frexp(amax, &e);
+  return e;
+}
+
+// One warp per row of A.
+__global__ void ozaki_row_exp_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols,
+                                     int32_t* __restrict__ ea) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = warp; r < rows; r += nwarps) {
+    double m = 0.0;
+    for (int c = lane; c < cols; c += 32) m = fmax(m, fabs(A[(int64_t)r * lda + c]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) ea[r] = exp_of(m);
+  }
+}
+
+// Column maxima of B (K x N): block of 32 x 8 threads covers 32 columns,
+// the 8 thread rows stride over K.
+__global__ void ozaki_col_exp_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols,
+                                     int32_t* __restrict__ eb) {
+  __shared__ double red[8][33];
+  const int n = blockIdx.x * 32 + threadIdx.x;
+  double m = 0.0;
+  if (n < ncols)
+    for (int k = threadIdx.y; k < krows; k += 8) m = fmax(m, fabs(B[(int64_t)k * ldb + n]));
+  red[threadIdx.y][threadIdx.x] = m;
+  __syncthreads();
+  if (threadIdx.y == 0 && n < ncols) {
+    for (int i = 1; i < 8; ++i) m = fmax(m, red[i][threadIdx.x]);
+    eb[n] = exp_of(m);
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
+  double r = ldexp(v, -e);
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    r = r * 128.0;
+    const double w = trunc(r);
+    q[t] = (int8_t)(int)w;
+    r = r - w;
+  }
+}
+
+// A rows -> [S][rows][kpad]; each thread slices 4 consecutive columns.
+template <int S>
+__global__ void ozaki_slice_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
+                                        const int32_t* __restrict__ ea, int8_t* __restrict__ out) {
+  const int64_t c4 = ceil_div(cols, 4);
+  const int64_t total = (int64_t)rows * c4;
+  const int64_t plane = (int64_t)rows * kpad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / c4;
+    const int c = (int)(idx - r * c4) * 4;
+    const int e = ea[r];
+    int8_t q[4][S];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double v = c + j < cols ? A[r * lda + c + j] : 0.0;
+      slice_value<S>(v, e, q[j]);
+    }
+    if (c + 4 <= kpad) {
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
+                            ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
+        *reinterpret_cast<uint32_t*>(out + t * plane + r * kpad + c) = pk;
+      }
+    }
+  }
+}
+
+// B (K x N) -> [S][N][kpad] transposed through a 32 x 32 tile (32 x 8 threads).
+template <int S>
+__global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
+                                        const int32_t* __restrict__ eb, int8_t* __restrict__ out) {
+  __shared__ double tile[32][33];
+  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
+  const int64_t plane = (int64_t)ncols * kpad;
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int k = k0 + i, n = n0 + threadIdx.x;
+    tile[i][threadIdx.x] = (k < krows && n < ncols) ? B[(int64_t)k * ldb + n] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += 8) {
+    const int n = n0 + i, k = k0 + threadIdx.x;
+    if (n < ncols && k < kpad) {
+      int8_t q[S];
+      slice_value<S>(tile[threadIdx.x][i], eb[n], q);
+#pragma unroll
+      for (int t = 0; t < S; ++t) out[t * plane + (int64_t)n * kpad + k] = q[t];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- launch
+static unsigned grid_for(int64_t work, int threads, int sms) {
+  int64_t b = ceil_div(work, threads);
+  b = std::min<int64_t>(b, (int64_t)sms * 16);
+  return (unsigned)std::max<int64_t>(b, 1);
+}
+
+cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
+                              bool transpose, int sms, cudaStream_t st) {
+  if (!transpose) {
+    split_bf16_rows_kernel<<<grid_for((int64_t)rows * ceil_div(cols, 4), 256, sms), 256, 0, st>>>(
+        A, lda, rows, cols, kpad, nterms, static_cast<__nv_bfloat16*>(out));
+  } else {
+    // A is K x N here (krows = rows, ncols = cols); output N x kpad.
+    dim3 grid((unsigned)ceil_div(cols, 32), (unsigned)ceil_div(kpad, 32));
+    split_bf16_cols_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, rows, cols, kpad, nterms,
+                                                         static_cast<__nv_bfloat16*>(out));
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
+                                   int32_t* ea, int32_t* eb, int sms, cudaStream_t st) {
+  ozaki_row_exp_kernel<<<grid_for((int64_t)m * 32, 256, sms), 256, 0, st>>>(A, lda, m, k, ea);
+  ozaki_col_exp_kernel<<<(unsigned)ceil_div(n, 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, eb);
+  return cudaGetLastError();
+}
+
+template <int S>
+static cudaError_t slices_s(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
+                            int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                            cudaStream_t st) {
+  ozaki_slice_rows_kernel<S><<<grid_for((int64_t)m * ceil_div(k, 4), 256, sms), 256, 0, st>>>(A, lda, m, k, kpad, ea,
+                                                                                               sa);
+  dim3 grid((unsigned)ceil_div(n, 32), (unsigned)ceil_div(kpad, 32));
+  ozaki_slice_cols_kernel<S><<<grid, dim3(32, 8), 0, st>>>(B, ldb, k, n, kpad, eb, sb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
+                                int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                                cudaStream_t st) {
+  switch (s) {
+    case 4: return slices_s<4>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 5: return slices_s<5>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 6: return slices_s<6>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 7: return slices_s<7>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 8: return slices_s<8>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 9: return slices_s<9>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace cucosma

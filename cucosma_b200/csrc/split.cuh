@@ -1,0 +1,26 @@
+// split.cuh -- launchers of the operand pre-passes (BF16 split, Ozaki slices).
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace cucosma {
+
+// FP32 rows x cols -> nterms BF16 planes.  transpose = false: planes are
+// [nterms][rows][kpad] (A operand, cols = K).  transpose = true: the input is
+// K x N (rows = K, cols = N) and planes are [nterms][N][kpad] (B operand).
+cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
+                              bool transpose, int sms, cudaStream_t st);
+
+// Per-row exponents of A (m x k) and per-column exponents of B (k x n).
+cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
+                                   int32_t* ea, int32_t* eb, int sms, cudaStream_t st);
+
+// s INT8 slices: sa [s][m][kpad], sb [s][n][kpad].
+cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
+                                int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                                cudaStream_t st);
+
+}  // namespace cucosma

@@ -1,13 +1,614 @@
-// tc_gemm.cu -- tensor-core precision paths (filled in below as they land).
+// tc_gemm.cu -- tcgen05 tensor-core GEMM for the precision paths.
+//
+// One persistent, warp-specialised kernel template serves both precision
+// forms that have no counterpart in the reference (which is FP32 SIMT only,
+// cuCOSMAV100.cuh:2505-2756):
+//
+//   BF16x3 / BF16x6 SGEMM   A = sum_i A_i, B = sum_j B_j (BF16 split planes);
+//                           C ~= sum over the kept (i, j) of A_i * B_j, all
+//                           products accumulated in one FP32 TMEM accumulator.
+//   Ozaki DGEMM (INT8)      A_p, B_q signed 7-bit slices; for every diagonal
+//                           d = p + q < s an exact INT32 TMEM accumulator
+//                           S_d = sum_{p+q=d} A_p * B_q; the epilogue
+//                           recombines sum_d S_d 2^(-7(d+2)) in FP64 (d
+//                           descending) and rescales by 2^(e_row + e_col).
+//
+// Roles (192 threads): warp 0 lane 0 streams the slice planes of A and B
+// with 3-D TMA loads (all planes of one k-block in one box) into a
+// multi-stage shared-memory ring; warp 1 allocates TMEM and one lane issues
+// tcgen05.mma (A and B from shared memory, K-major, swizzled) and commits to
+// mbarriers; warps 2-5 drain the accumulators (tcgen05.ld), apply
+// alpha/beta and the fused epilogue and store through a shared-memory
+// transpose for coalesced rows.  Accumulators are double-buffered in TMEM
+// when they fit, so the epilogue of one tile overlaps the next tile's MMAs.
+// Work units (tile x K split) are distributed round-robin over a persistent
+// grid with a banded raster (the reference's block swizzle,
+// cuCOSMAV100.cuh:2586-2603, generalised).  Split-K writes raw partials to
+// the workspace and a separate kernel reduces them in split order.
+//
+// Every mbarrier wait is bounded (ptx.cuh); on expiry the roles leave their
+// loops, drain what they issued, and TMEM is released before exit.
+#include <cuda_bf16.h>
+
 #include "api_internal.cuh"
+#include "simt_gemm.cuh"
+#include "split.cuh"
+#include "tc_gemm.cuh"
 
 namespace cucosma {
-cucosma_status tc_workspace_size(const cucosma_gemm_desc*, size_t* bytes, const DeviceInfo*) {
-  *bytes = 0;
-  return CUCOSMA_STATUS_NOT_SUPPORTED;
+namespace tc {
+
+// Shared-memory matrix descriptor, K-major operand written by TMA with a
+// swizzle span of SWZ bytes per row: start >> 4 at [0,14), leading byte
+// offset (unused for swizzled K-major) at [16,30), stride byte offset
+// (8 rows x SWZ) >> 4 at [32,46), version 1 at [46,48), layout type at
+// [61,64): 2 = 128B, 4 = 64B, 6 = 32B swizzle.
+template <int SWZ>
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  constexpr uint64_t layout = SWZ == 128 ? 2 : (SWZ == 64 ? 4 : 6);
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)((8 * SWZ) >> 4) << 32) |
+         ((uint64_t)1 << 46) | (layout << 61);
 }
-cucosma_status tc_gemm(const cucosma_gemm_desc*, const void*, const void*, void*, void*, const DeviceInfo*,
-                       cudaStream_t) {
-  return CUCOSMA_STATUS_NOT_SUPPORTED;
+
+__device__ __forceinline__ void unit_coords(int unit, int tiles, int tiles_m, int tiles_n, int band, int& z, int& tm,
+                                            int& tn) {
+  z = unit / tiles;
+  const int t = unit - z * tiles;
+  const int per_band = band * tiles_n;
+  const int b = t / per_band;
+  const int w = t - b * per_band;
+  const int rows = min(band, tiles_m - b * band);
+  tm = b * band + w % rows;
+  tn = w / rows;
 }
+
+template <class Tr>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+  constexpr int BN = Tr::BN, SWZ = Tr::SWZ, NA = Tr::NA, NB = Tr::NB, NACC = Tr::NACC, ST = Tr::STAGES;
+  constexpr int A_TILE = 128 * SWZ, B_TILE = BN * SWZ;
+  constexpr int STAGE_BYTES = NA * A_TILE + NB * B_TILE;
+  constexpr int KSTEPS = SWZ / 32;  // MMAs per plane pair per stage (32 bytes of K each)
+  constexpr int NBUF = Tr::NBUF;
+  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, BN) : idesc_bf16_f32(128, BN);
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* stages = smem;
+  uint8_t* staging = smem + ST * STAGE_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + Tr::STAGING_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + ST;
+  uint64_t* tfull = bars + 2 * ST;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tiles = p.tiles_m * p.tiles_n;
+  const int units = tiles * p.splits;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_init(drain, 1);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_holder, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if (lane == 0) {
+      tma_prefetch_desc(&tmA);
+      tma_prefetch_desc(&tmB);
+      int it = 0;  // global k-block counter (ring position)
+      bool ok = true;
+      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+        int z, tm, tn;
+        unit_coords(unit, tiles, p.tiles_m, p.tiles_n, p.band, z, tm, tn);
+        const int kb0 = z * p.kb_per_split, kb1 = min(p.kblocks, kb0 + p.kb_per_split);
+        for (int kb = kb0; kb < kb1; ++kb, ++it) {
+          const int s = it % ST;
+          if (!mbar_wait(&empty[s], ((it / ST) & 1) ^ 1, kErrTimeoutEmpty, p.ctl)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = stages + s * STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+          tma_load_3d(st, &tmA, kb * Tr::BK, tm * 128, 0, &full[s]);
+          tma_load_3d(st + NA * A_TILE, &tmB, kb * Tr::BK, tn * BN, 0, &full[s]);
+        }
+      }
+      if (!ok)  // drain loads that may still be in flight (bounded)
+        for (int j = max(0, it - ST); j < it; ++j) mbar_wait(&full[j % ST], (j / ST) & 1, kErrTimeoutDrain, p.ctl);
+    }
+  } else if (warp == 1) {
+    // -------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int it = 0, i = 0;
+      bool ok = true;
+      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x, ++i) {
+        int z, tm, tn;
+        unit_coords(unit, tiles, p.tiles_m, p.tiles_n, p.band, z, tm, tn);
+        const int kb0 = z * p.kb_per_split, kb1 = min(p.kblocks, kb0 + p.kb_per_split);
+        const int buf = i % NBUF;
+        if (!mbar_wait(&tempty[buf], ((i / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc0 = tmem_base + (uint32_t)(buf * NACC * BN);
+        for (int kb = kb0; kb < kb1; ++kb, ++it) {
+          const int s = it % ST;
+          if (!mbar_wait(&full[s], (it / ST) & 1, kErrTimeoutFull, p.ctl)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
+          const uint32_t b_base = a_base + NA * A_TILE;
+#pragma unroll
+          for (int t = 0; t < Tr::NT; ++t) {
+#pragma unroll
+            for (int kk = 0; kk < KSTEPS; ++kk) {
+              const uint64_t ad = sdesc<SWZ>(a_base + Tr::ta(t) * A_TILE + kk * 32);
+              const uint64_t bd = sdesc<SWZ>(b_base + Tr::tb(t) * B_TILE + kk * 32);
+              const bool acc = !(kb == kb0 && kk == 0 && Tr::first_for_acc(t));
+              const uint32_t d = acc0 + (uint32_t)(Tr::td(t) * BN);
+              if (Tr::kInt8)
+                mma_i8(d, ad, bd, IDESC, acc);
+              else
+                mma_bf16(d, ad, bd, IDESC, acc);
+            }
+          }
+          mma_commit(&empty[s]);  // stage free once these MMAs have read it
+        }
+        if (!ok) break;
+        mma_commit(&tfull[buf]);  // accumulator ready once every MMA above completes
+      }
+      if (!ok) {
+        mma_commit(drain);  // wait (bounded) for every MMA issued so far
+        mbar_wait(drain, 0, kErrTimeoutDrain, p.ctl);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quadrant this warp may access
+    const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
+    int i = 0;
+    for (int unit = blockIdx.x; unit < units; unit += gridDim.x, ++i) {
+      int z, tm, tn;
+      unit_coords(unit, tiles, p.tiles_m, p.tiles_n, p.band, z, tm, tn);
+      const int buf = i % NBUF;
+      bool ok = mbar_wait(&tfull[buf], (i / NBUF) & 1, kErrTimeoutAccum, p.ctl);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      const int row0 = tm * 128 + 32 * q;
+      const int col0 = tn * BN;
+      Tr::epilogue(p, lane_base + (uint32_t)(buf * NACC * BN), staging + (warp - 2) * Tr::STAGING_PER_WARP, lane,
+                   row0, col0, z);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[buf]);
+    }
+  }
+
+  tc_fence_before();
+  __syncwarp();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// ------------------------------------------------------------ epilogues
+// FP32 result (BF16 split paths).  Each warp owns 32 rows; chunks of 32
+// columns go TMEM -> registers -> padded shared tile -> coalesced rows.
+struct EpiF32 {
+  static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
+  template <int BN>
+  static __device__ __forceinline__ void run(const TcParams& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
+                                             int col0, int z) {
+    float* stg = reinterpret_cast<float*>(stg_raw);
+    const float alpha = (float)p.alpha, beta = (float)p.beta;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t v0[16], v1[16];
+      tmem_ld16(tacc + c0, v0);
+      tmem_ld16(tacc + c0 + 16, v1);
+      tmem_ld_wait();
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        stg[lane * 33 + j] = __uint_as_float(v0[j]);
+        stg[lane * 33 + 16 + j] = __uint_as_float(v1[j]);
+      }
+      __syncwarp();
+      const int col = col0 + c0 + lane;
+      if (col < p.n) {
+        if (p.partial) {
+          float* w = reinterpret_cast<float*>(p.out) + (int64_t)z * p.ws_split_stride + col;
+#pragma unroll 4
+          for (int r = 0; r < 32; ++r) {
+            const int row = row0 + r;
+            if (row < p.m) w[(int64_t)row * p.ldo] = stg[r * 33 + lane];
+          }
+        } else {
+          float* o = reinterpret_cast<float*>(p.out) + col;
+#pragma unroll 4
+          for (int r = 0; r < 32; ++r) {
+            const int row = row0 + r;
+            if (row < p.m) {
+              float* po = o + (int64_t)row * p.ldo;
+              *po = apply_epi(combine(stg[r * 33 + lane], alpha, beta, po), p.epilogue);
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+};
+
+// FP64 result (Ozaki).  Chunks of 16 columns: part = sum_{d = S-1..0}
+// S_d * 2^(-7(d+2)) (FP64, d descending), then 2^(e_row + e_col) and
+// alpha/beta; or the raw part into the split-K workspace.
+template <int S>
+struct EpiOzaki {
+  static constexpr int STAGING_PER_WARP = 32 * 17 * 8;
+  template <int BN>
+  static __device__ __forceinline__ void run(const TcParams& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
+                                             int col0, int z) {
+    double* stg = reinterpret_cast<double*>(stg_raw);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      double part[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) part[j] = 0.0;
+#pragma unroll
+      for (int d = S - 1; d >= 0; --d) {
+        uint32_t v[16];
+        tmem_ld16(tacc + d * BN + c0, v);
+        tmem_ld_wait();
+        const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+        for (int j = 0; j < 16; ++j) part[j] = part[j] + (double)(int32_t)v[j] * w;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = part[j];
+      __syncwarp();
+      const int cl = lane & 15;
+      const int col = col0 + c0 + cl;
+      if (col < p.n) {
+        const int ecol = p.partial ? 0 : p.eb[col];
+#pragma unroll 4
+        for (int h = 0; h < 16; ++h) {
+          const int r = (lane >> 4) + 2 * h;
+          const int row = row0 + r;
+          if (row >= p.m) continue;
+          const double v = stg[r * 17 + cl];
+          if (p.partial) {
+            reinterpret_cast<double*>(p.out)[(int64_t)z * p.ws_split_stride + (int64_t)row * p.ldo + col] = v;
+          } else {
+            double* po = reinterpret_cast<double*>(p.out) + (int64_t)row * p.ldo + col;
+            const double r_ = ldexp(v, p.ea[row] + ecol);
+            const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * *po);
+            *po = apply_epi(o, p.epilogue);
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+};
+
+// ------------------------------------------------------------- traits
+constexpr int kSmemBudget = 227 * 1024;
+
+template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi>
+struct TraitsBase {
+  static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
+  static constexpr bool kInt8 = INT8_;
+  static constexpr int BK = SWZ / (INT8_ ? 1 : 2);
+  static constexpr int NBUF = (2 * NACC * BN <= 512) ? 2 : 1;
+  static constexpr int STAGING_PER_WARP = Epi::STAGING_PER_WARP;
+  static constexpr int STAGING_BYTES = 4 * STAGING_PER_WARP;
+  static constexpr int STAGE_BYTES = (NA * 128 + NB * BN) * SWZ;
+  static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
+  static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
+  static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
+  static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
+  static_assert(STAGES >= 2, "at least a double-buffered ring");
+  static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
+  static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
+  static __device__ __forceinline__ void epilogue(const TcParams& p, uint32_t tacc, uint8_t* stg, int lane, int row0,
+                                                  int col0, int z) {
+    Epi::template run<BN>(p, tacc, stg, lane, row0, col0, z);
+  }
+};
+
+// BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
+struct Bf16x3 : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32> {
+  static constexpr __device__ int ta(int t) { return t == 0 ? 1 : 0; }
+  static constexpr __device__ int tb(int t) { return t == 1 ? 1 : 0; }
+  static constexpr __device__ int td(int) { return 0; }
+  static constexpr __device__ bool first_for_acc(int t) { return t == 0; }
+};
+
+// BF16x6: 3-way split, the six products with i + j <= 2, small terms first.
+struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 1, false, EpiF32> {
+  static constexpr __device__ int ta(int t) { return t == 0 ? 2 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 1 : 0; }
+  static constexpr __device__ int tb(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 2 : t == 3 ? 0 : t == 4 ? 1 : 0; }
+  static constexpr __device__ int td(int) { return 0; }
+  static constexpr __device__ bool first_for_acc(int t) { return t == 0; }
+};
+// term 5 is (0,0): ta(5) = 0, tb(5) = 0.
+
+// Ozaki with S slices: all pairs (p, q) with p + q < S, ordered by p then q;
+// accumulator d = p + q; BN chosen so that S accumulators fit in TMEM.
+template <int S>
+struct OzakiBN {
+  static constexpr int value = S <= 8 ? 64 : (S <= 10 ? 48 : 32);
+};
+template <int S>
+struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 32, S, S, S, true, EpiOzaki<S>> {
+  // term t -> (p, q): enumerate p = 0.., q = 0..S-1-p
+  static constexpr __device__ int pq(int t, bool want_p) {
+    int p = 0;
+    while (t >= S - p) {
+      t -= S - p;
+      ++p;
+    }
+    return want_p ? p : t;
+  }
+  static constexpr __device__ int ta(int t) { return pq(t, true); }
+  static constexpr __device__ int tb(int t) { return pq(t, false); }
+  static constexpr __device__ int td(int t) { return pq(t, true) + pq(t, false); }
+  // first term writing diagonal d is (0, d): p == 0
+  static constexpr __device__ bool first_for_acc(int t) { return pq(t, true) == 0; }
+};
+
+template <class Tr>
+static cudaError_t launch(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p, int grid, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tr::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  tc_gemm_kernel<Tr><<<grid, kThreads, Tr::SMEM, st>>>(a, b, p);
+  return cudaGetLastError();
+}
+
+// Split-K reduction of the Ozaki path: tot = sum_z ws[z] (z ascending),
+// C = epi(alpha * ldexp(tot, ea + eb) + beta * C).
+__global__ void ozaki_reduce_kernel(const double* __restrict__ ws, int64_t split_stride, int64_t ldw, int splits,
+                                    double* C, int64_t ldc, int m, int n, const int32_t* __restrict__ ea,
+                                    const int32_t* __restrict__ eb, double alpha, double beta, int epi) {
+  const int64_t total = (int64_t)m * n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / n;
+    const int c = (int)(idx - r * n);
+    const double* w = ws + r * ldw + c;
+    double tot = w[0];
+    for (int zz = 1; zz < splits; ++zz) tot = tot + w[zz * split_stride];
+    const double v = ldexp(tot, ea[r] + eb[c]);
+    double* po = C + r * ldc + c;
+    const double o = beta == 0.0 ? alpha * v : fma(alpha, v, beta * *po);
+    *po = apply_epi(o, epi);
+  }
+}
+
+// ------------------------------------------------------------ planning
+struct Plan {
+  int kind;  // 0 bf16x3, 1 bf16x6, 2 ozaki
+  int slices, bn, bk, tiles_m, tiles_n, kblocks, kb_per_split, splits, band;
+  int64_t kpad;
+  size_t off_a, off_b, off_ea, off_eb, off_part, bytes;
+  int64_t ldw;
+};
+
+static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
+  Plan pl{};
+  const int64_t M = d->m, N = d->n, K = d->k;
+  if (d->precision == CUCOSMA_PRECISION_OZAKI) {
+    pl.kind = 2;
+    pl.slices = d->slices ? d->slices : kOzakiDefaultSlices;
+    pl.bn = pl.slices <= 8 ? 64 : (pl.slices <= 10 ? 48 : 32);
+    pl.bk = 32;
+    pl.kpad = round_up(K, 16);
+  } else {
+    pl.kind = d->precision == CUCOSMA_PRECISION_BF16X6 ? 1 : 0;
+    pl.slices = pl.kind == 1 ? 3 : 2;
+    pl.bn = pl.kind == 1 ? 128 : 256;
+    pl.bk = 32;
+    pl.kpad = round_up(K, 8);
+  }
+  pl.tiles_m = (int)ceil_div(M, 128);
+  pl.tiles_n = (int)ceil_div(N, pl.bn);
+  pl.kblocks = (int)ceil_div(K, pl.bk);
+  const int64_t tiles = (int64_t)pl.tiles_m * pl.tiles_n;
+  int64_t min_splits = 1;
+  if (pl.kind == 2) {
+    // Exact INT32 diagonals: slices * kchunk * 127^2 < 2^31.
+    const int64_t kmax = ((int64_t)2147483647 / ((int64_t)pl.slices * 127 * 127)) / pl.bk * pl.bk;
+    min_splits = ceil_div(K, kmax);
+  }
+  int64_t splits = d->split_k > 0 ? d->split_k : 1;
+  if (d->split_k <= 0 && tiles < di->sms) splits = std::max<int64_t>(1, std::min<int64_t>(di->sms / tiles, pl.kblocks / 16));
+  splits = std::max(splits, min_splits);
+  splits = std::min<int64_t>(splits, pl.kblocks);
+  pl.kb_per_split = (int)ceil_div(pl.kblocks, splits);
+  if (pl.kind == 2) {
+    const int64_t kbmax = ((int64_t)2147483647 / ((int64_t)pl.slices * 127 * 127)) / pl.bk;
+    pl.kb_per_split = (int)std::min<int64_t>(pl.kb_per_split, kbmax);
+  }
+  pl.splits = (int)ceil_div(pl.kblocks, pl.kb_per_split);
+  pl.band = d->swizzle > 0 ? d->swizzle : 8;
+  const int es_in = pl.kind == 2 ? 1 : 2;
+  const int es_out = pl.kind == 2 ? 8 : 4;
+  size_t off = 0;
+  pl.off_a = off;
+  off = al256(off + (size_t)pl.slices * M * pl.kpad * es_in);
+  pl.off_b = off;
+  off = al256(off + (size_t)pl.slices * N * pl.kpad * es_in);
+  pl.off_ea = off;
+  if (pl.kind == 2) {
+    off = al256(off + (size_t)M * 4);
+    pl.off_eb = off;
+    off = al256(off + (size_t)N * 4);
+  }
+  pl.ldw = round_up(N, 4);
+  pl.off_part = off;
+  if (pl.splits > 1) off = al256(off + (size_t)pl.splits * M * pl.ldw * es_out);
+  pl.bytes = off;
+  return pl;
+}
+
+}  // namespace tc
+
+// ------------------------------------------------------------ host API
+using namespace tc;
+
+cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const DeviceInfo* di) {
+  *bytes = make_plan(d, di).bytes;
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
+void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info) {
+  const Plan pl = make_plan(d, di);
+  info->path = pl.kind + 1;
+  info->tile_m = 128;
+  info->tile_n = pl.bn;
+  info->tile_k = pl.bk;
+  info->splits = pl.splits;
+  info->band = pl.band;
+  info->slices = pl.slices;
+  info->launches = (pl.kind == 2 ? 5 : 3) + (pl.splits > 1 ? 1 : 0);
+  info->kchunk = (int64_t)pl.kb_per_split * pl.bk;
+  info->kpad = pl.kpad;
+  info->workspace_bytes = pl.bytes;
+  info->off_a = pl.off_a;
+  info->off_b = pl.off_b;
+  info->off_ea = pl.off_ea;
+  info->off_eb = pl.off_eb;
+  info->off_part = pl.off_part;
+}
+
+cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
+                       const DeviceInfo* di, cudaStream_t st) {
+  const Plan pl = make_plan(d, di);
+  if (pl.kind == 2 && (pl.slices < 4 || pl.slices > 9)) return CUCOSMA_STATUS_NOT_SUPPORTED;
+  uint8_t* w = static_cast<uint8_t*>(ws);
+  const int m = (int)d->m, n = (int)d->n, k = (int)d->k;
+  TcParams p{};
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.tiles_m = pl.tiles_m;
+  p.tiles_n = pl.tiles_n;
+  p.kblocks = pl.kblocks;
+  p.kb_per_split = pl.kb_per_split;
+  p.splits = pl.splits;
+  p.band = pl.band;
+  p.epilogue = d->epilogue;
+  p.alpha = d->alpha;
+  p.beta = d->beta;
+  wait_ctl(di, &p.ctl.status, &p.ctl.timeout_ns);
+  if (pl.splits > 1) {
+    p.partial = 1;
+    p.out = w + pl.off_part;
+    p.ldo = pl.ldw;
+    p.ws_split_stride = (int64_t)m * pl.ldw;
+  } else {
+    p.partial = 0;
+    p.out = C;
+    p.ldo = d->ldc;
+  }
+  const int units = pl.tiles_m * pl.tiles_n * pl.splits;
+  const int grid = std::min(units, di->sms);
+  CUtensorMap ta, tb;
+  cudaError_t e = cudaSuccess;
+  int launches = 0;
+  if (pl.kind != 2) {
+    const int nt = pl.slices;
+    e = launch_split_bf16((const float*)A, d->lda, m, k, pl.kpad, nt, w + pl.off_a, false, di->sms, st);
+    if (e == cudaSuccess)
+      e = launch_split_bf16((const float*)B, d->ldb, k, n, pl.kpad, nt, w + pl.off_b, true, di->sms, st);
+    launches += 2;
+    if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, w + pl.off_a, k, m, nt, pl.kpad, (uint64_t)m * pl.kpad,
+                   pl.bk, 128, nt, CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, w + pl.off_b, k, n, nt, pl.kpad, (uint64_t)n * pl.kpad,
+                   pl.bk, pl.bn, nt, CU_TENSOR_MAP_SWIZZLE_64B))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    prof_begin(st);
+    e = pl.kind == 0 ? launch<Bf16x3>(ta, tb, p, grid, st) : launch<Bf16x6>(ta, tb, p, grid, st);
+    prof_end(st);
+    launches += 1;
+    if (e == cudaSuccess && pl.splits > 1) {
+      e = simt::launch_reduce<float>((const float*)p.out, p.ws_split_stride, pl.ldw, pl.splits, (float*)C, d->ldc, m, n,
+                                     d->alpha, d->beta, d->epilogue, di->sms, st);
+      launches += 1;
+    }
+  } else {
+    const int s = pl.slices;
+    int32_t* ea = reinterpret_cast<int32_t*>(w + pl.off_ea);
+    int32_t* eb = reinterpret_cast<int32_t*>(w + pl.off_eb);
+    e = launch_ozaki_exponents((const double*)A, d->lda, (const double*)B, d->ldb, m, n, k, ea, eb, di->sms, st);
+    if (e == cudaSuccess)
+      e = launch_ozaki_slices(s, (const double*)A, d->lda, (const double*)B, d->ldb, m, n, k, pl.kpad, ea, eb,
+                              reinterpret_cast<int8_t*>(w + pl.off_a), reinterpret_cast<int8_t*>(w + pl.off_b),
+                              di->sms, st);
+    launches += 4;
+    if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_a, k, m, s, pl.kpad, (uint64_t)m * pl.kpad, pl.bk,
+                   128, s, CU_TENSOR_MAP_SWIZZLE_32B) ||
+        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_b, k, n, s, pl.kpad, (uint64_t)n * pl.kpad, pl.bk,
+                   pl.bn, s, CU_TENSOR_MAP_SWIZZLE_32B))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    p.ea = ea;
+    p.eb = eb;
+    prof_begin(st);
+    switch (s) {
+      case 4: e = launch<Ozaki<4>>(ta, tb, p, grid, st); break;
+      case 5: e = launch<Ozaki<5>>(ta, tb, p, grid, st); break;
+      case 6: e = launch<Ozaki<6>>(ta, tb, p, grid, st); break;
+      case 7: e = launch<Ozaki<7>>(ta, tb, p, grid, st); break;
+      case 8: e = launch<Ozaki<8>>(ta, tb, p, grid, st); break;
+      case 9: e = launch<Ozaki<9>>(ta, tb, p, grid, st); break;
+      default: return CUCOSMA_STATUS_NOT_SUPPORTED;
+    }
+    prof_end(st);
+    launches += 1;
+    if (e == cudaSuccess && pl.splits > 1) {
+      const int64_t work = (int64_t)m * n;
+      const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(work, 256), di->sms * 8));
+      ozaki_reduce_kernel<<<blocks, 256, 0, st>>>((const double*)p.out, p.ws_split_stride, pl.ldw, pl.splits,
+                                                  (double*)C, d->ldc, m, n, ea, eb, d->alpha, d->beta, d->epilogue);
+      e = cudaGetLastError();
+      launches += 1;
+    }
+  }
+  note_launches(launches);
+  return e == cudaSuccess ? CUCOSMA_STATUS_SUCCESS : CUCOSMA_STATUS_LAUNCH_FAILED;
+}
+
 }  // namespace cucosma

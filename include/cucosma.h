@@ -87,6 +87,23 @@ CUCOSMA_API void cucosma_gemm_desc_init(cucosma_gemm_desc* d);
 /* Bytes of device workspace cucosma_gemm needs for *d (0 when none). */
 CUCOSMA_API cucosma_status cucosma_gemm_workspace_size(const cucosma_gemm_desc* d, size_t* bytes);
 
+/* The execution plan cucosma_gemm would use for *d on the current device:
+ * the compile-time tiling of config.h (THREADBLOCK_TILE_M/N, LOAD_K,
+ * SPLIT_K, SWIZZLE) as chosen at run time, plus the workspace layout of the
+ * precision paths (offsets of the operand planes inside the workspace). */
+typedef struct cucosma_plan_info {
+  int32_t path;     /* 0 native SIMT, 1 BF16x3, 2 BF16x6, 3 Ozaki */
+  int32_t tile_m, tile_n, tile_k;
+  int32_t splits;   /* split-K factor */
+  int32_t band;     /* raster band / block-index remap width */
+  int32_t slices;   /* operand planes (BF16 terms or Ozaki slices) */
+  int32_t launches; /* kernels one cucosma_gemm call enqueues */
+  int64_t kchunk;   /* K extent of one split */
+  int64_t kpad;     /* padded K of the operand planes */
+  uint64_t workspace_bytes, off_a, off_b, off_ea, off_eb, off_part;
+} cucosma_plan_info;
+CUCOSMA_API cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cucosma_plan_info* info);
+
 /* C = epi(alpha*A*B + beta*C).  workspace may be NULL when the size is 0.
  * Allocation-free; asynchronous on stream.  Replaces cosmaSgemm
  * (cuCOSMAV100.cuh:2774-2848) including its split-K workspace path

@@ -1,0 +1,220 @@
+"""GPU parity tests of the tensor-core precision paths through the C ABI.
+
+BF16x3 / BF16x6 SGEMM: the BF16 split planes are checked bit for bit against
+the oracle's split restatement, and results against the FP64 oracle within
+the bound of the split (stated in each test).  Ozaki DGEMM: exponents, INT8
+slices and the final FP64 result are checked bit for bit against the
+oracle's restatement (integer products are exact, the recombination order is
+fixed), and the error against a double-double oracle is stated."""
+import numpy as np
+import pytest
+
+import cucosma_b200 as cc
+import oracle
+from tests._util import expspread, to_dev, uniform
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def short_waits(cuda):
+    # A broken barrier protocol shows up as a TIMEOUT status within 2 s.
+    cc.set_wait_timeout_ns(2_000_000_000)
+    yield
+    s, code = cc.device_status()
+    assert s == cc.SUCCESS, "device status %d code 0x%x" % (s, code)
+
+
+def run(A, B, Cin, alpha, beta, precision, epilogue="none", slices=0, split_k=0, keep_ws=False):
+    import torch
+
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(Cin)
+    d = cc.make_desc(dA, dB, dC, alpha, beta, precision=precision, epilogue=epilogue, slices=slices, split_k=split_k)
+    plan = cc.get_plan(d)
+    ws = cc.alloc_workspace(d)
+    cc.gemm(dA, dB, dC, alpha, beta, precision=precision, epilogue=epilogue, slices=slices, split_k=split_k,
+            workspace=ws)
+    torch.cuda.synchronize()
+    out = dC.cpu().numpy()
+    if keep_ws:
+        return out, plan, (ws.cpu().numpy() if ws is not None else None)
+    return out, plan
+
+
+def bf16_bound(A, B, Cin, alpha, beta, nterms):
+    """|err| <= (c_split + 6 (k+2) u32) |alpha| (|A||B|) + 2 u32 |beta C| + 2 u32 |result|,
+    c_split = 3.1 * 2^-16 for BF16x3 (dropped lo*lo and the two residuals),
+    6 * 2^-24 for BF16x6."""
+    k = A.shape[1]
+    u = 2.0 ** -24
+    c_split = 3.1 * 2.0 ** -16 if nterms == 2 else 6.0 * u
+    absab = oracle.gemm(np.abs(A), np.abs(B))
+    ref = oracle.gemm(A, B, Cin, alpha, beta)
+    b = (c_split + 6 * (k + 2) * u) * abs(alpha) * absab + 2 * u * np.abs(ref) + 1e-30
+    if beta:
+        b += 2 * u * abs(beta) * np.abs(Cin.astype(np.float64))
+    return ref, b
+
+
+SHAPES = [(1, 1, 1), (7, 5, 3), (128, 256, 32), (129, 257, 33), (300, 200, 100), (256, 512, 1024), (1000, 64, 77),
+          (64, 1000, 2000)]
+
+
+@pytest.mark.parametrize("precision,nterms", [("bf16x3", 2), ("bf16x6", 3)])
+def test_split_planes_bitexact(precision, nterms):
+    m, n, k = 130, 70, 45
+    A = uniform(1, (m, k))
+    B = uniform(2, (k, n))
+    Cin = np.zeros((m, n), np.float32)
+    _, plan, ws = run(A, B, Cin, 1.0, 0.0, precision, keep_ws=True)
+    kpad = plan["kpad"]
+    raw = ws.view(np.uint16)
+    pa = raw[plan["off_a"] // 2: plan["off_a"] // 2 + nterms * m * kpad].reshape(nterms, m, kpad)[:, :, :k]
+    pb = raw[plan["off_b"] // 2: plan["off_b"] // 2 + nterms * n * kpad].reshape(nterms, n, kpad)[:, :, :k]
+    assert np.array_equal(pa, oracle.split_bf16(A, nterms))
+    assert np.array_equal(pb, oracle.split_bf16(np.ascontiguousarray(B.T), nterms))
+
+
+@pytest.mark.parametrize("precision,nterms", [("bf16x3", 2), ("bf16x6", 3)])
+@pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d" % s for s in SHAPES])
+def test_bf16_paths_vs_oracle(precision, nterms, shape):
+    m, n, k = shape
+    A = uniform(3, (m, k))
+    B = uniform(4, (k, n))
+    Cin = uniform(5, (m, n))
+    out, plan = run(A, B, Cin, 1.0, 0.5, precision)
+    ref, b = bf16_bound(A, B, Cin, 1.0, 0.5, nterms)
+    err = np.abs(out.astype(np.float64) - ref)
+    assert np.all(err <= b), (plan, oracle.errors(out, ref), float((err / b).max()))
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("split_k", [2, 5])
+def test_bf16_split_k(precision, split_k):
+    A = uniform(6, (200, 3000))
+    B = uniform(7, (3000, 300))
+    Cin = uniform(8, (200, 300))
+    out, plan = run(A, B, Cin, 1.5, -0.5, precision, split_k=split_k)
+    assert plan["splits"] == split_k
+    ref, b = bf16_bound(A, B, Cin, 1.5, -0.5, 2 if precision == "bf16x3" else 3)
+    assert np.all(np.abs(out - ref) <= b)
+
+
+@pytest.mark.parametrize("epi,code", [("sigmoid", oracle.EPI_SIGMOID), ("relu", oracle.EPI_RELU)])
+def test_bf16x3_fused_epilogue(epi, code):
+    A = uniform(9, (257, 130), lo=-0.3, hi=0.3)
+    B = uniform(10, (130, 300), lo=-0.3, hi=0.3)
+    Cin = uniform(11, (257, 300))
+    out, _ = run(A, B, Cin, 1.0, 0.5, "bf16x3", epilogue=epi)
+    pre, b = bf16_bound(A, B, Cin, 1.0, 0.5, 2)
+    ref = oracle.gemm(A, B, Cin, 1.0, 0.5, code)
+    lip = 0.25 if code == oracle.EPI_SIGMOID else 1.0
+    assert np.all(np.abs(out - ref) <= lip * b + 8 * 2.0 ** -24)
+
+
+def test_bf16x6_not_worse_than_native_fp32():
+    m, n, k = 512, 512, 4096
+    A = uniform(12, (m, k))
+    B = uniform(13, (k, n))
+    Cin = np.zeros((m, n), np.float32)
+    ref = oracle.gemm(A, B)
+    e6 = oracle.errors(run(A, B, Cin, 1.0, 0.0, "bf16x6")[0], ref)
+    e3 = oracle.errors(run(A, B, Cin, 1.0, 0.0, "bf16x3")[0], ref)
+    en = oracle.errors(run(A, B, Cin, 1.0, 0.0, "native")[0], ref)
+    print("errors vs FP64: native", en, "bf16x3", e3, "bf16x6", e6)
+    assert e6["normwise"] <= en["normwise"] * 1.5
+
+
+def test_bf16_deterministic():
+    A = uniform(14, (300, 2000))
+    B = uniform(15, (2000, 260))
+    Cin = uniform(16, (300, 260))
+    outs = [run(A, B, Cin, 1.0, 0.5, "bf16x3", split_k=3)[0] for _ in range(3)]
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+# ------------------------------------------------------------------ Ozaki
+
+
+@pytest.mark.parametrize("dist", ["uniform", "expspread"])
+def test_ozaki_slices_bitexact(dist):
+    m, n, k, s = 70, 90, 100, 7
+    A = uniform(20, (m, k), np.float64) if dist == "uniform" else expspread(20, (m, k))
+    B = uniform(21, (k, n), np.float64) if dist == "uniform" else expspread(21, (k, n))
+    Cin = np.zeros((m, n))
+    _, plan, ws = run(A, B, Cin, 1.0, 0.0, "ozaki", slices=s, keep_ws=True)
+    kpad = plan["kpad"]
+    ea, eb, sa, sb = oracle.ozaki_slices(A, B, s)
+    g_ea = ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32)
+    g_eb = ws[plan["off_eb"]: plan["off_eb"] + 4 * n].view(np.int32)
+    g_sa = ws[plan["off_a"]: plan["off_a"] + s * m * kpad].view(np.int8).reshape(s, m, kpad)[:, :, :k]
+    g_sb = ws[plan["off_b"]: plan["off_b"] + s * n * kpad].view(np.int8).reshape(s, n, kpad)[:, :, :k]
+    assert np.array_equal(g_ea, ea) and np.array_equal(g_eb, eb)
+    assert np.array_equal(g_sa, sa) and np.array_equal(g_sb, sb)
+
+
+OZ_SHAPES = [(1, 1, 1), (7, 5, 3), (128, 64, 32), (129, 65, 33), (300, 200, 100), (256, 256, 1024), (1000, 48, 77)]
+
+
+@pytest.mark.parametrize("s", [6, 7, 8, 9])
+@pytest.mark.parametrize("shape", OZ_SHAPES, ids=["%dx%dx%d" % x for x in OZ_SHAPES])
+def test_ozaki_bitexact_vs_restatement(shape, s):
+    m, n, k = shape
+    A = uniform(22, (m, k), np.float64)
+    B = uniform(23, (k, n), np.float64)
+    Cin = uniform(24, (m, n), np.float64)
+    out, plan = run(A, B, Cin, 1.25, 0.5, "ozaki", slices=s)
+    kchunk = plan["kchunk"] if plan["splits"] > 1 else 0
+    ref = oracle.ozaki_gemm(A, B, s, Cin=Cin, alpha=1.25, beta=0.5, kchunk=kchunk)
+    assert np.array_equal(out, ref), (plan, oracle.errors(out, ref))
+
+
+@pytest.mark.parametrize("split_k", [2, 3, 8])
+def test_ozaki_split_k_bitexact(split_k):
+    A = expspread(25, (150, 2000))
+    B = expspread(26, (2000, 100))
+    Cin = uniform(27, (150, 100), np.float64)
+    out, plan = run(A, B, Cin, 1.0, -1.0, "ozaki", slices=8, split_k=split_k)
+    assert plan["splits"] == split_k
+    ref = oracle.ozaki_gemm(A, B, 8, Cin=Cin, alpha=1.0, beta=-1.0, kchunk=plan["kchunk"])
+    assert np.array_equal(out, ref)
+
+
+def test_ozaki_accuracy_vs_double_double():
+    A = uniform(28, (256, 2048), np.float64)
+    B = uniform(29, (2048, 192), np.float64)
+    Cin = np.zeros((256, 192))
+    hi, lo = oracle.gemm(A, B, dd=True)
+    res = {}
+    for s in (6, 7, 8, 9):
+        out, _ = run(A, B, Cin, 1.0, 0.0, "ozaki", slices=s)
+        res[s] = oracle.errors(out, hi, lo)
+    nat, _ = run(A, B, Cin, 1.0, 0.0, "native")
+    res["native"] = oracle.errors(nat, hi, lo)
+    print("Ozaki vs double-double:", res)
+    assert res[8]["normwise"] <= 1e-15
+    assert res[8]["normwise"] <= res["native"]["normwise"]
+
+
+def test_ozaki_sigmoid_epilogue():
+    A = uniform(30, (100, 64), np.float64, -0.2, 0.2)
+    B = uniform(31, (64, 80), np.float64, -0.2, 0.2)
+    Cin = uniform(32, (100, 80), np.float64)
+    out, _ = run(A, B, Cin, 1.0, 0.5, "ozaki", epilogue="sigmoid", slices=8)
+    ref = oracle.gemm(A, B, Cin, 1.0, 0.5, oracle.EPI_SIGMOID)
+    assert oracle.errors(out, ref)["max_rel"] < 1e-14
+
+
+def test_plan_reports_launches():
+    import torch
+
+    A = to_dev(uniform(33, (256, 256)))
+    B = to_dev(uniform(34, (256, 256)))
+    Cm = to_dev(np.zeros((256, 256), np.float32))
+    for prec in ("native", "bf16x3", "bf16x6"):
+        d = cc.make_desc(A, B, Cm, precision=prec)
+        plan = cc.get_plan(d)
+        n0 = cc.launch_count()
+        cc.gemm(A, B, Cm, precision=prec)
+        torch.cuda.synchronize()
+        assert cc.launch_count() - n0 == plan["launches"]
