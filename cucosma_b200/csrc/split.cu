@@ -9,7 +9,8 @@
 // Ozaki slicing (INT8 DGEMM): per row of A / per column of B the exponent
 // e with |x| < 2^e over the row / column; x * 2^-e is cut into s signed
 // 7-bit integer slices q_t = trunc(r * 2^7), r <- r * 2^7 - q_t, exact in
-// FP64.  A slices [s][M][kpad], B slices [s][N][kpad] (transposed).
+// FP64.  Slices of A rows and of B columns (B transposed) are stored packed
+// (see packed_index), kpad = K rounded up to the 32-wide k-block.
 //
 // All pre-passes are HBM-bound elementwise / transpose kernels.
 #include <cuda_bf16.h>
@@ -142,13 +143,22 @@ __device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
   }
 }
 
-// A rows -> [S][rows][kpad]; each thread slices 4 consecutive columns.
+// Packed slice layout shared by both operands: for row r (a row of A, or a
+// column of B), k-block kb = k / 32 and slice p, the 32 bytes of k-block kb
+// of slice p are at r * (kpad * S) + kb * (32 * S) + p * 32.  Four slices of
+// one k-block thus fill one 128-byte row, the span of the 128-byte swizzle
+// the tensor cores read, and one TMA box row is 128 contiguous bytes.
+template <int S>
+__device__ __forceinline__ int64_t packed_index(int64_t r, int k, int64_t kpad, int p) {
+  return r * (kpad * S) + (int64_t)(k >> 5) * (32 * S) + p * 32 + (k & 31);
+}
+
+// A rows -> packed slices; each thread slices 4 consecutive columns.
 template <int S>
 __global__ void ozaki_slice_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
                                         const int32_t* __restrict__ ea, int8_t* __restrict__ out) {
-  const int64_t c4 = ceil_div(cols, 4);
+  const int64_t c4 = kpad / 4;
   const int64_t total = (int64_t)rows * c4;
-  const int64_t plane = (int64_t)rows * kpad;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = idx / c4;
@@ -160,24 +170,22 @@ __global__ void ozaki_slice_rows_kernel(const double* __restrict__ A, int64_t ld
       const double v = c + j < cols ? A[r * lda + c + j] : 0.0;
       slice_value<S>(v, e, q[j]);
     }
-    if (c + 4 <= kpad) {
 #pragma unroll
-      for (int t = 0; t < S; ++t) {
-        const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
-                            ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
-        *reinterpret_cast<uint32_t*>(out + t * plane + r * kpad + c) = pk;
-      }
+    for (int t = 0; t < S; ++t) {
+      const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
+                          ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
+      *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, kpad, t)) = pk;
     }
   }
 }
 
-// B (K x N) -> [S][N][kpad] transposed through a 32 x 32 tile (32 x 8 threads).
+// B (K x N) -> packed slices of its columns, through a 32 x 32 tile
+// (32 x 8 threads); a tile row covers one k-block.
 template <int S>
 __global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
                                         const int32_t* __restrict__ eb, int8_t* __restrict__ out) {
   __shared__ double tile[32][33];
   const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
-  const int64_t plane = (int64_t)ncols * kpad;
   for (int i = threadIdx.y; i < 32; i += 8) {
     const int k = k0 + i, n = n0 + threadIdx.x;
     tile[i][threadIdx.x] = (k < krows && n < ncols) ? B[(int64_t)k * ldb + n] : 0.0;
@@ -189,7 +197,7 @@ __global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ld
       int8_t q[S];
       slice_value<S>(tile[threadIdx.x][i], eb[n], q);
 #pragma unroll
-      for (int t = 0; t < S; ++t) out[t * plane + (int64_t)n * kpad + k] = q[t];
+      for (int t = 0; t < S; ++t) out[packed_index<S>(n, k, kpad, t)] = q[t];
     }
   }
 }
@@ -226,8 +234,8 @@ template <int S>
 static cudaError_t slices_s(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
                             int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
                             cudaStream_t st) {
-  ozaki_slice_rows_kernel<S><<<grid_for((int64_t)m * ceil_div(k, 4), 256, sms), 256, 0, st>>>(A, lda, m, k, kpad, ea,
-                                                                                               sa);
+  ozaki_slice_rows_kernel<S><<<grid_for((int64_t)m * (kpad / 4), 256, sms), 256, 0, st>>>(A, lda, m, k, kpad, ea,
+                                                                                           sa);
   dim3 grid((unsigned)ceil_div(n, 32), (unsigned)ceil_div(kpad, 32));
   ozaki_slice_cols_kernel<S><<<grid, dim3(32, 8), 0, st>>>(B, ldb, k, n, kpad, eb, sb);
   return cudaGetLastError();

@@ -18,7 +18,9 @@ cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, i
 cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
                                    int32_t* ea, int32_t* eb, int sms, cudaStream_t st);
 
-// s INT8 slices: sa [s][m][kpad], sb [s][n][kpad].
+// s INT8 slices of the rows of A and of the columns of B, packed (four
+// slices' 32-byte k-blocks per 128-byte row): byte (r, k, p) at
+// r * kpad * s + (k / 32) * 32 * s + p * 32 + k % 32; kpad a multiple of 32.
 cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
                                 int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
                                 cudaStream_t st);

@@ -30,6 +30,8 @@
 // loops, drain what they issued, and TMEM is released before exit.
 #include <cuda_bf16.h>
 
+#include <utility>
+
 #include "api_internal.cuh"
 #include "simt_gemm.cuh"
 #include "split.cuh"
@@ -62,13 +64,38 @@ __device__ __forceinline__ void unit_coords(int unit, int tiles, int tiles_m, in
   tn = w / rows;
 }
 
+// Issues the MMAs of term T for one stage.  Descriptor start addresses
+// advance by compile-time offsets (>> 4, no carry out of the 14-bit field
+// since every operand lies inside shared memory).
+template <class Tr, int T>
+__device__ __forceinline__ void issue_term(uint64_t ad0, uint64_t bd0, uint32_t acc0, bool not_first_kb) {
+  constexpr int KSTEPS = Tr::KSTEPS;
+  constexpr int PA = Tr::kTerms.a[T], PB = Tr::kTerms.b[T], D = Tr::kTerms.d[T];
+  constexpr bool FIRST = Tr::kTerms.first[T];
+  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, Tr::BN) : idesc_bf16_f32(128, Tr::BN);
+#pragma unroll
+  for (int kk = 0; kk < KSTEPS; ++kk) {
+    const uint64_t ad = ad0 + (uint64_t)(Tr::a_off(PA, kk) >> 4);
+    const uint64_t bd = bd0 + (uint64_t)(Tr::b_off(PB, kk) >> 4);
+    const bool acc = (FIRST && kk == 0) ? not_first_kb : true;
+    if constexpr (Tr::kInt8)
+      mma_i8(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+    else
+      mma_bf16(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+  }
+}
+template <class Tr, int... Ts>
+__device__ __forceinline__ void issue_terms(std::integer_sequence<int, Ts...>, uint64_t ad0, uint64_t bd0, uint32_t acc0,
+                                            bool not_first_kb) {
+  (issue_term<Tr, Ts>(ad0, bd0, acc0, not_first_kb), ...);
+}
+
 template <class Tr>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
   constexpr int BN = Tr::BN, SWZ = Tr::SWZ, NA = Tr::NA, NB = Tr::NB, NACC = Tr::NACC, ST = Tr::STAGES;
-  constexpr int A_TILE = 128 * SWZ, B_TILE = BN * SWZ;
-  constexpr int STAGE_BYTES = NA * A_TILE + NB * B_TILE;
-  constexpr int KSTEPS = SWZ / 32;  // MMAs per plane pair per stage (32 bytes of K each)
+  constexpr int A_REGION = Tr::A_REGION;
+  constexpr int STAGE_BYTES = Tr::STAGE_BYTES;
   constexpr int NBUF = Tr::NBUF;
   constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, BN) : idesc_bf16_f32(128, BN);
 
@@ -128,8 +155,18 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           uint8_t* st = stages + s * STAGE_BYTES;
           mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-          tma_load_3d(st, &tmA, kb * Tr::BK, tm * 128, 0, &full[s]);
-          tma_load_3d(st + NA * A_TILE, &tmB, kb * Tr::BK, tn * BN, 0, &full[s]);
+          if constexpr (Tr::PACKED) {
+            // boxes of [rows][128 B]: slices 4j..4j+3 of k-block kb
+#pragma unroll
+            for (int j = 0; j < Tr::TILES_A; ++j) tma_load_3d(st + j * Tr::A_TILE, &tmA, j * 128, kb, tm * 128, &full[s]);
+#pragma unroll
+            for (int j = 0; j < Tr::TILES_B; ++j)
+              tma_load_3d(st + A_REGION + j * Tr::B_TILE, &tmB, j * 128, kb, tn * BN, &full[s]);
+          } else {
+            // one box of [planes][rows][BK] per operand
+            tma_load_3d(st, &tmA, kb * Tr::BK, tm * 128, 0, &full[s]);
+            tma_load_3d(st + A_REGION, &tmB, kb * Tr::BK, tn * BN, 0, &full[s]);
+          }
         }
       }
       if (!ok)  // drain loads that may still be in flight (bounded)
@@ -159,21 +196,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           tc_fence_after();
           const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
-          const uint32_t b_base = a_base + NA * A_TILE;
-#pragma unroll
-          for (int t = 0; t < Tr::NT; ++t) {
-#pragma unroll
-            for (int kk = 0; kk < KSTEPS; ++kk) {
-              const uint64_t ad = sdesc<SWZ>(a_base + Tr::ta(t) * A_TILE + kk * 32);
-              const uint64_t bd = sdesc<SWZ>(b_base + Tr::tb(t) * B_TILE + kk * 32);
-              const bool acc = !(kb == kb0 && kk == 0 && Tr::first_for_acc(t));
-              const uint32_t d = acc0 + (uint32_t)(Tr::td(t) * BN);
-              if (Tr::kInt8)
-                mma_i8(d, ad, bd, IDESC, acc);
-              else
-                mma_bf16(d, ad, bd, IDESC, acc);
-            }
-          }
+          const uint64_t ad0 = sdesc<SWZ>(a_base);
+          const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
+          issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != kb0);
           mma_commit(&empty[s]);  // stage free once these MMAs have read it
         }
         if (!ok) break;
@@ -319,15 +344,32 @@ struct EpiOzaki {
 // ------------------------------------------------------------- traits
 constexpr int kSmemBudget = 227 * 1024;
 
+// Stage layout.  Unpacked (BF16 planes): one tile of rows x SWZ bytes per
+// plane, KSTEPS MMAs of 32 bytes of K each per plane pair.  Packed (Ozaki
+// INT8 slices): one stage is one 32-wide k-block; four slices share each
+// 128-byte swizzled row, so slice p sits in tile p / 4 at byte offset
+// (p % 4) * 32 -- selected like a K offset inside the swizzle atom.
 template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi>
 struct TraitsBase {
   static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
   static constexpr bool kInt8 = INT8_;
-  static constexpr int BK = SWZ / (INT8_ ? 1 : 2);
+  static constexpr bool PACKED = INT8_;
+  static constexpr int BK = PACKED ? 32 : SWZ / 2;  // K elements per stage
+  static constexpr int KSTEPS = PACKED ? 1 : SWZ / 32;
+  static constexpr int TILES_A = PACKED ? (NA + 3) / 4 : NA;  // TMA boxes per operand per stage
+  static constexpr int TILES_B = PACKED ? (NB + 3) / 4 : NB;
+  static constexpr int A_TILE = 128 * SWZ, B_TILE = BN * SWZ;
+  static constexpr int A_REGION = TILES_A * A_TILE;
+  static constexpr __host__ __device__ int a_off(int p, int kk) {
+    return PACKED ? (p / 4) * A_TILE + (p % 4) * 32 : p * A_TILE + kk * 32;
+  }
+  static constexpr __host__ __device__ int b_off(int q, int kk) {
+    return PACKED ? (q / 4) * B_TILE + (q % 4) * 32 : q * B_TILE + kk * 32;
+  }
   static constexpr int NBUF = (2 * NACC * BN <= 512) ? 2 : 1;
   static constexpr int STAGING_PER_WARP = Epi::STAGING_PER_WARP;
   static constexpr int STAGING_BYTES = 4 * STAGING_PER_WARP;
-  static constexpr int STAGE_BYTES = (NA * 128 + NB * BN) * SWZ;
+  static constexpr int STAGE_BYTES = TILES_A * A_TILE + TILES_B * B_TILE;
   static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
   static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
   static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
@@ -342,44 +384,51 @@ struct TraitsBase {
 };
 
 // BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
+// Term tables: for term t, the A plane a[t], the B plane b[t], the
+// accumulator d[t], and whether t is the first term of the k-block order to
+// write accumulator d[t] (that MMA overwrites instead of accumulating on the
+// first k-block of a unit).  Built at compile time.
+template <int NT>
+struct TermTable {
+  int a[NT], b[NT], d[NT];
+  bool first[NT];
+};
+
+// BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
 struct Bf16x3 : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32> {
-  static constexpr __device__ int ta(int t) { return t == 0 ? 1 : 0; }
-  static constexpr __device__ int tb(int t) { return t == 1 ? 1 : 0; }
-  static constexpr __device__ int td(int) { return 0; }
-  static constexpr __device__ bool first_for_acc(int t) { return t == 0; }
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
 };
 
 // BF16x6: 3-way split, the six products with i + j <= 2, small terms first.
 struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 1, false, EpiF32> {
-  static constexpr __device__ int ta(int t) { return t == 0 ? 2 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 1 : 0; }
-  static constexpr __device__ int tb(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 2 : t == 3 ? 0 : t == 4 ? 1 : 0; }
-  static constexpr __device__ int td(int) { return 0; }
-  static constexpr __device__ bool first_for_acc(int t) { return t == 0; }
+  static constexpr TermTable<6> kTerms{
+      {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {0, 0, 0, 0, 0, 0}, {true, false, false, false, false, false}};
 };
-// term 5 is (0,0): ta(5) = 0, tb(5) = 0.
 
 // Ozaki with S slices: all pairs (p, q) with p + q < S, ordered by p then q;
-// accumulator d = p + q; BN chosen so that S accumulators fit in TMEM.
+// accumulator d = p + q (the first writer of diagonal d is (0, d)); BN chosen
+// so that S accumulators fit in TMEM.
 template <int S>
 struct OzakiBN {
   static constexpr int value = S <= 8 ? 64 : (S <= 10 ? 48 : 32);
 };
 template <int S>
-struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 32, S, S, S, true, EpiOzaki<S>> {
-  // term t -> (p, q): enumerate p = 0.., q = 0..S-1-p
-  static constexpr __device__ int pq(int t, bool want_p) {
-    int p = 0;
-    while (t >= S - p) {
-      t -= S - p;
-      ++p;
+constexpr TermTable<S*(S + 1) / 2> ozaki_terms() {
+  TermTable<S*(S + 1) / 2> t{};
+  int i = 0;
+  for (int p = 0; p < S; ++p)
+    for (int q = 0; p + q < S; ++q) {
+      t.a[i] = p;
+      t.b[i] = q;
+      t.d[i] = p + q;
+      t.first[i] = p == 0;
+      ++i;
     }
-    return want_p ? p : t;
-  }
-  static constexpr __device__ int ta(int t) { return pq(t, true); }
-  static constexpr __device__ int tb(int t) { return pq(t, false); }
-  static constexpr __device__ int td(int t) { return pq(t, true) + pq(t, false); }
-  // first term writing diagonal d is (0, d): p == 0
-  static constexpr __device__ bool first_for_acc(int t) { return pq(t, true) == 0; }
+  return t;
+}
+template <int S>
+struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, EpiOzaki<S>> {
+  static constexpr TermTable<S*(S + 1) / 2> kTerms = ozaki_terms<S>();
 };
 
 template <class Tr>
@@ -433,7 +482,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
     pl.slices = d->slices ? d->slices : kOzakiDefaultSlices;
     pl.bn = pl.slices <= 8 ? 64 : (pl.slices <= 10 ? 48 : 32);
     pl.bk = 32;
-    pl.kpad = round_up(K, 16);
+    pl.kpad = round_up(K, 32);
   } else {
     pl.kind = d->precision == CUCOSMA_PRECISION_BF16X6 ? 1 : 0;
     pl.slices = pl.kind == 1 ? 3 : 2;
@@ -579,10 +628,12 @@ cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B,
                               di->sms, st);
     launches += 4;
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
-    if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_a, k, m, s, pl.kpad, (uint64_t)m * pl.kpad, pl.bk,
-                   128, s, CU_TENSOR_MAP_SWIZZLE_32B) ||
-        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_b, k, n, s, pl.kpad, (uint64_t)n * pl.kpad, pl.bk,
-                   pl.bn, s, CU_TENSOR_MAP_SWIZZLE_32B))
+    // Packed slices as a 3-D byte tensor {32 s (slices of one k-block), k-blocks, rows}.
+    const uint64_t kbs = (uint64_t)pl.kpad / 32;
+    if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_a, 32ull * s, kbs, m, 32ull * s,
+                   (uint64_t)pl.kpad * s, 128, 1, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_b, 32ull * s, kbs, n, 32ull * s,
+                   (uint64_t)pl.kpad * s, 128, 1, pl.bn, CU_TENSOR_MAP_SWIZZLE_128B))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     p.ea = ea;
     p.eb = eb;

@@ -122,7 +122,7 @@ def test_bf16x6_not_worse_than_native_fp32():
     e3 = oracle.errors(run(A, B, Cin, 1.0, 0.0, "bf16x3")[0], ref)
     en = oracle.errors(run(A, B, Cin, 1.0, 0.0, "native")[0], ref)
     print("errors vs FP64: native", en, "bf16x3", e3, "bf16x6", e6)
-    assert e6["normwise"] <= en["normwise"] * 1.5
+    assert e6["normwise"] <= e3["normwise"]
 
 
 def test_bf16_deterministic():
@@ -147,10 +147,15 @@ def test_ozaki_slices_bitexact(dist):
     ea, eb, sa, sb = oracle.ozaki_slices(A, B, s)
     g_ea = ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32)
     g_eb = ws[plan["off_eb"]: plan["off_eb"] + 4 * n].view(np.int32)
-    g_sa = ws[plan["off_a"]: plan["off_a"] + s * m * kpad].view(np.int8).reshape(s, m, kpad)[:, :, :k]
-    g_sb = ws[plan["off_b"]: plan["off_b"] + s * n * kpad].view(np.int8).reshape(s, n, kpad)[:, :, :k]
+    def unpack(off, rows):
+        # packed layout: [rows][k-block][slice][32 bytes] -> [slice][rows][k]
+        raw = ws[off: off + s * rows * kpad].view(np.int8).reshape(rows, kpad // 32, s, 32)
+        return raw.transpose(2, 0, 1, 3).reshape(s, rows, kpad)
+
+    g_sa, g_sb = unpack(plan["off_a"], m), unpack(plan["off_b"], n)
     assert np.array_equal(g_ea, ea) and np.array_equal(g_eb, eb)
-    assert np.array_equal(g_sa, sa) and np.array_equal(g_sb, sb)
+    assert np.array_equal(g_sa[:, :, :k], sa) and np.array_equal(g_sb[:, :, :k], sb)
+    assert not g_sa[:, :, k:].any() and not g_sb[:, :, k:].any()  # K padding is zero
 
 
 OZ_SHAPES = [(1, 1, 1), (7, 5, 3), (128, 64, 32), (129, 65, 33), (300, 200, 100), (256, 256, 1024), (1000, 48, 77)]
