@@ -121,6 +121,24 @@ CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
                              double beta, double* C, int ldc, void* stream);
 
+/* Allocation-free FP32 split-K GEMM.  No counterpart in the reference (whose
+ * split-K path cudaMallocs its workspace on every call).  For callers that
+ * must not allocate device memory -- e.g. a plugin whose host framework owns
+ * the whole device pool, or a latency-critical caller that cannot afford
+ * cudaMalloc's implicit synchronisation.  Same arithmetic as cucosma_sgemm
+ * with SPLIT_K = split_k (0 = library choice); the split-K partial sums live
+ * in a fixed device array of CUCOSMA_STATIC_SCRATCH_BYTES inside the library,
+ * held by every device that loads it until the process exits.  Problems whose
+ * partials (splits * m * round_up(n, 4) floats) exceed it return
+ * CUCOSMA_STATUS_WORKSPACE_TOO_SMALL without launching.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, and must be ordered by the caller. */
+#define CUCOSMA_STATIC_SCRATCH_BYTES (16u << 20)
+CUCOSMA_API cucosma_status cucosma_sgemm_splitk_static(int m, int n, int k, float alpha, const float* A, int lda,
+                                                       const float* B, int ldb, float beta, float* C, int ldc,
+                                                       int split_k, void* stream);
+
 /* Synchronises the device, then returns and clears the device status word:
  * CUCOSMA_STATUS_TIMEOUT if any kernel gave up on a bounded wait since the
  * last call, CUCOSMA_STATUS_LAUNCH_FAILED on a CUDA error, else SUCCESS.
