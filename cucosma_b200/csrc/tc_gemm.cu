@@ -107,20 +107,25 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* full = bars;
   uint64_t* empty = bars + ST;
   uint64_t* tfull = bars + 2 * ST;
-  uint64_t* tempty = tfull + 2;
-  uint64_t* drain = tempty + 2;
+  uint64_t* tempty = tfull + 4;
+  uint64_t* drain = tempty + 4;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  static_assert(NBUF <= 4, "accumulator buffers");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles = p.tiles_m * p.tiles_n;
   const int units = tiles * p.splits;
+  // K-blocks per accumulator chunk: with promotion the tensor cores
+  // accumulate CHUNK k-blocks in TMEM and the epilogue warps add each chunk
+  // into FP32 registers (round to nearest); otherwise one chunk per unit.
+  const int chunk = Tr::PROMOTE ? Tr::CHUNK : p.kblocks;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 4; ++b) {
       mbar_init(&tfull[b], 1);
       mbar_init(&tempty[b], 4);
     }
@@ -175,34 +180,37 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     // -------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      int it = 0, i = 0;
+      int it = 0, ci = 0;
       bool ok = true;
-      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x, ++i) {
+      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
         int z, tm, tn;
         unit_coords(unit, tiles, p.tiles_m, p.tiles_n, p.band, z, tm, tn);
         const int kb0 = z * p.kb_per_split, kb1 = min(p.kblocks, kb0 + p.kb_per_split);
-        const int buf = i % NBUF;
-        if (!mbar_wait(&tempty[buf], ((i / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t acc0 = tmem_base + (uint32_t)(buf * NACC * BN);
-        for (int kb = kb0; kb < kb1; ++kb, ++it) {
-          const int s = it % ST;
-          if (!mbar_wait(&full[s], (it / ST) & 1, kErrTimeoutFull, p.ctl)) {
+        for (int cs = kb0; cs < kb1 && ok; cs += chunk, ++ci) {
+          const int ce = min(kb1, cs + chunk);
+          const int buf = ci % NBUF;
+          if (!mbar_wait(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
-          const uint64_t ad0 = sdesc<SWZ>(a_base);
-          const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
-          issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != kb0);
-          mma_commit(&empty[s]);  // stage free once these MMAs have read it
+          const uint32_t acc0 = tmem_base + (uint32_t)(buf * NACC * BN);
+          for (int kb = cs; kb < ce; ++kb, ++it) {
+            const int s = it % ST;
+            if (!mbar_wait(&full[s], (it / ST) & 1, kErrTimeoutFull, p.ctl)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
+            const uint64_t ad0 = sdesc<SWZ>(a_base);
+            const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
+            issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != cs);
+            mma_commit(&empty[s]);  // stage free once these MMAs have read it
+          }
+          if (!ok) break;
+          mma_commit(&tfull[buf]);  // accumulator ready once every MMA above completes
         }
-        if (!ok) break;
-        mma_commit(&tfull[buf]);  // accumulator ready once every MMA above completes
       }
       if (!ok) {
         mma_commit(drain);  // wait (bounded) for every MMA issued so far
@@ -213,22 +221,42 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------- epilogue
     const int q = warp & 3;  // TMEM lane quadrant this warp may access
     const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
-    int i = 0;
-    for (int unit = blockIdx.x; unit < units; unit += gridDim.x, ++i) {
+    uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
+    int ci = 0;
+    bool ok = true;
+    for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
       int z, tm, tn;
       unit_coords(unit, tiles, p.tiles_m, p.tiles_n, p.band, z, tm, tn);
-      const int buf = i % NBUF;
-      bool ok = mbar_wait(&tfull[buf], (i / NBUF) & 1, kErrTimeoutAccum, p.ctl);
-      ok = __all_sync(0xffffffffu, ok);
-      if (!ok) break;
-      tc_fence_after();
       const int row0 = tm * 128 + 32 * q;
       const int col0 = tn * BN;
-      Tr::epilogue(p, lane_base + (uint32_t)(buf * NACC * BN), staging + (warp - 2) * Tr::STAGING_PER_WARP, lane,
-                   row0, col0, z);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[buf]);
+      if constexpr (Tr::PROMOTE) {
+        const int kb0 = z * p.kb_per_split, kb1 = min(p.kblocks, kb0 + p.kb_per_split);
+        float master[BN];
+#pragma unroll
+        for (int j = 0; j < BN; ++j) master[j] = 0.f;
+        for (int cs = kb0; cs < kb1; cs += chunk, ++ci) {
+          const int buf = ci % NBUF;
+          ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
+          if (!ok) break;
+          tc_fence_after();
+          Tr::accumulate(lane_base + (uint32_t)(buf * NACC * BN), master);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        if (!ok) break;
+        Tr::finish(p, master, stg, lane, row0, col0, z);
+      } else {
+        const int buf = ci % NBUF;
+        ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
+        if (!ok) break;
+        tc_fence_after();
+        Tr::epilogue(p, lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        ++ci;
+      }
     }
   }
 
@@ -246,11 +274,37 @@ __global__ void __launch_bounds__(kThreads, 1)
 // columns go TMEM -> registers -> padded shared tile -> coalesced rows.
 struct EpiF32 {
   static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
+
+  // Stores the 32 x 32 block staged in stg (row r of the warp's rows in
+  // stg[r * 33 + ...]) at columns col0 + c0 + [0, 32): coalesced rows.
+  static __device__ __forceinline__ void store32(const TcParams& p, const float* stg, int lane, int row0, int col,
+                                                 int z) {
+    if (col >= p.n) return;
+    if (p.partial) {
+      float* w = reinterpret_cast<float*>(p.out) + (int64_t)z * p.ws_split_stride + col;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = row0 + r;
+        if (row < p.m) w[(int64_t)row * p.ldo] = stg[r * 33 + lane];
+      }
+    } else {
+      const float alpha = (float)p.alpha, beta = (float)p.beta;
+      float* o = reinterpret_cast<float*>(p.out) + col;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = row0 + r;
+        if (row < p.m) {
+          float* po = o + (int64_t)row * p.ldo;
+          *po = apply_epi(combine(stg[r * 33 + lane], alpha, beta, po), p.epilogue);
+        }
+      }
+    }
+  }
+
   template <int BN>
   static __device__ __forceinline__ void run(const TcParams& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
                                              int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
-    const float alpha = (float)p.alpha, beta = (float)p.beta;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t v0[16], v1[16];
@@ -263,27 +317,44 @@ struct EpiF32 {
         stg[lane * 33 + 16 + j] = __uint_as_float(v1[j]);
       }
       __syncwarp();
-      const int col = col0 + c0 + lane;
-      if (col < p.n) {
-        if (p.partial) {
-          float* w = reinterpret_cast<float*>(p.out) + (int64_t)z * p.ws_split_stride + col;
-#pragma unroll 4
-          for (int r = 0; r < 32; ++r) {
-            const int row = row0 + r;
-            if (row < p.m) w[(int64_t)row * p.ldo] = stg[r * 33 + lane];
-          }
-        } else {
-          float* o = reinterpret_cast<float*>(p.out) + col;
-#pragma unroll 4
-          for (int r = 0; r < 32; ++r) {
-            const int row = row0 + r;
-            if (row < p.m) {
-              float* po = o + (int64_t)row * p.ldo;
-              *po = apply_epi(combine(stg[r * 33 + lane], alpha, beta, po), p.epilogue);
-            }
-          }
+      store32(p, stg, lane, row0, col0 + c0 + lane, z);
+      __syncwarp();
+    }
+  }
+
+  // Promotion: add one chunk's TMEM accumulators (this thread's row, BN
+  // columns each; the correction products' accumulator NACC-1 first, the
+  // main product's accumulator 0 last) into the FP32 register accumulator,
+  // rounding to nearest.
+  template <int BN, int NACC>
+  static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[BN]) {
+#pragma unroll
+    for (int d = NACC - 1; d >= 0; --d) {
+#pragma unroll
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t v0[16], v1[16];
+        tmem_ld16(tacc + d * BN + c0, v0);
+        tmem_ld16(tacc + d * BN + c0 + 16, v1);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          master[c0 + j] = __fadd_rn(master[c0 + j], __uint_as_float(v0[j]));
+          master[c0 + 16 + j] = __fadd_rn(master[c0 + 16 + j], __uint_as_float(v1[j]));
         }
       }
+    }
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void finish(const TcParams& p, const float (&master)[BN], uint8_t* stg_raw,
+                                                int lane, int row0, int col0, int z) {
+    float* stg = reinterpret_cast<float*>(stg_raw);
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = master[c0 + j];
+      __syncwarp();
+      store32(p, stg, lane, row0, col0 + c0 + lane, z);
       __syncwarp();
     }
   }
@@ -349,10 +420,13 @@ constexpr int kSmemBudget = 227 * 1024;
 // INT8 slices): one stage is one 32-wide k-block; four slices share each
 // 128-byte swizzled row, so slice p sits in tile p / 4 at byte offset
 // (p % 4) * 32 -- selected like a K offset inside the swizzle atom.
-template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi>
+template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi, bool PROMOTE_ = false,
+          int CHUNK_ = 0>
 struct TraitsBase {
   static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
   static constexpr bool kInt8 = INT8_;
+  static constexpr bool PROMOTE = PROMOTE_;
+  static constexpr int CHUNK = CHUNK_;
   static constexpr bool PACKED = INT8_;
   static constexpr int BK = PACKED ? 32 : SWZ / 2;  // K elements per stage
   static constexpr int KSTEPS = PACKED ? 1 : SWZ / 32;
@@ -366,7 +440,8 @@ struct TraitsBase {
   static constexpr __host__ __device__ int b_off(int q, int kk) {
     return PACKED ? (q / 4) * B_TILE + (q % 4) * 32 : q * B_TILE + kk * 32;
   }
-  static constexpr int NBUF = (2 * NACC * BN <= 512) ? 2 : 1;
+  static constexpr int NBUF =
+      PROMOTE ? (512 / (NACC * BN) > 4 ? 4 : 512 / (NACC * BN)) : ((2 * NACC * BN <= 512) ? 2 : 1);
   static constexpr int STAGING_PER_WARP = Epi::STAGING_PER_WARP;
   static constexpr int STAGING_BYTES = 4 * STAGING_PER_WARP;
   static constexpr int STAGE_BYTES = TILES_A * A_TILE + TILES_B * B_TILE;
@@ -377,11 +452,23 @@ struct TraitsBase {
   static_assert(STAGES >= 2, "at least a double-buffered ring");
   static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
   static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
+  static_assert(!PROMOTE || (CHUNK > 0 && NBUF >= 2), "promotion needs chunk buffers");
   static __device__ __forceinline__ void epilogue(const TcParams& p, uint32_t tacc, uint8_t* stg, int lane, int row0,
                                                   int col0, int z) {
     Epi::template run<BN>(p, tacc, stg, lane, row0, col0, z);
   }
+  static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[BN]) {
+    if constexpr (PROMOTE) Epi::template accumulate<BN, NACC>(tacc, master);
+  }
+  static __device__ __forceinline__ void finish(const TcParams& p, const float (&master)[BN], uint8_t* stg, int lane,
+                                                int row0, int col0, int z) {
+    if constexpr (PROMOTE) Epi::template finish<BN>(p, master, stg, lane, row0, col0, z);
+  }
 };
+
+// K-blocks (32 wide) the tensor cores accumulate before the epilogue adds
+// the chunk into its FP32 registers.
+constexpr int kPromoteChunk = 4;
 
 // BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
 // Term tables: for term t, the A plane a[t], the B plane b[t], the
@@ -395,14 +482,24 @@ struct TermTable {
 };
 
 // BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
+// Default (tile id 0): 128 x 256 tiles, the whole K accumulated in one TMEM
+// accumulator -- the error of BF16x3 is set by its split, not by the
+// accumulation.  Tile id 2: 128 x 128 tiles with promotion, the correction
+// products in their own accumulator.
 struct Bf16x3 : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32> {
   static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
 };
+struct Bf16x3Promoted : TraitsBase<3, 128, 64, 2, 2, 2, false, EpiF32, true, kPromoteChunk> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {true, false, true}};
+};
 
-// BF16x6: 3-way split, the six products with i + j <= 2, small terms first.
-struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 1, false, EpiF32> {
+// BF16x6: 3-way split, the six products with i + j <= 2; the five
+// correction products accumulate in TMEM accumulator 1, the main product
+// hi*hi in accumulator 0, so the main accumulator is rounded only by its own
+// MMAs; both are promoted into FP32 registers every kPromoteChunk k-blocks.
+struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk> {
   static constexpr TermTable<6> kTerms{
-      {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {0, 0, 0, 0, 0, 0}, {true, false, false, false, false, false}};
+      {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
 // Ozaki with S slices: all pairs (p, q) with p + q < S, ordered by p then q;
@@ -486,7 +583,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
   } else {
     pl.kind = d->precision == CUCOSMA_PRECISION_BF16X6 ? 1 : 0;
     pl.slices = pl.kind == 1 ? 3 : 2;
-    pl.bn = pl.kind == 1 ? 128 : 256;
+    pl.bn = (pl.kind == 0 && d->tile != 2) ? 256 : 128;  // BF16x3 tile 2: promoted 128 x 128
     pl.bk = 32;
     pl.kpad = round_up(K, 8);
   }
@@ -609,7 +706,8 @@ cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B,
                    pl.bk, pl.bn, nt, CU_TENSOR_MAP_SWIZZLE_64B))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     prof_begin(st);
-    e = pl.kind == 0 ? launch<Bf16x3>(ta, tb, p, grid, st) : launch<Bf16x6>(ta, tb, p, grid, st);
+    e = pl.kind == 1 ? launch<Bf16x6>(ta, tb, p, grid, st)
+        : (pl.bn == 256 ? launch<Bf16x3>(ta, tb, p, grid, st) : launch<Bf16x3Promoted>(ta, tb, p, grid, st));
     prof_end(st);
     launches += 1;
     if (e == cudaSuccess && pl.splits > 1) {
