@@ -54,7 +54,7 @@ def peaks():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples (every 200 ms) of SM clock and throttle reasons."""
+    """nvidia-smi samples (every 50 ms) of SM clock and throttle reasons."""
 
     FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
@@ -68,7 +68,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -87,22 +87,25 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
+        sm, loaded, mx, reasons = [], [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
+                clk, mx, pw = float(parts[0]), float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[4:8]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+            sm.append(clk)
+            if pw > 250.0:  # samples taken while a kernel was running
+                loaded.append(clk)
+                for nm, v in zip(names, parts[4:8]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        use = loaded or sm
+        return {"sm_mhz": float(np.median(use)) if use else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm), "samples_under_load": len(loaded)}
 
 
 # ------------------------------------------------------------ distributed
@@ -201,6 +204,74 @@ def e2e_path(cc, A_h, B_h, C_h, A, B, Cm, prec, slices, steps, warmup, workspace
     e1.record(st)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / steps
+
+
+def grouped_shapes(count=512, seed=5):
+    """512 GEMMs: M, N log-uniform in [64, 2048], K log-uniform in [64, 8192]."""
+    r = np.random.default_rng(seed)
+    lu = lambda a, b: int(np.exp(r.uniform(np.log(a), np.log(b))))  # noqa: E731
+    return [(lu(64, 2048), lu(64, 2048), lu(64, 8192)) for _ in range(count)]
+
+
+def grouped_bench(cc, precision, dtype, slices, steps, warmup, seed=5):
+    """One persistent grouped launch (captured in a CUDA graph) against the
+    same 512 problems as 512 separate calls of the single-problem path (also
+    captured, so neither side pays Python launch overhead)."""
+    import torch
+
+    shapes = grouped_shapes(seed=seed)
+    flop = sum(2.0 * m * n * k for m, n, k in shapes)
+    es = torch.tensor([], dtype=dtype).element_size()
+    al = 16 // es
+
+    def rows(g, r, c):
+        return (torch.rand((r, -(-c // al) * al), generator=g, device="cuda", dtype=dtype) * 2 - 1)[:, :c]
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    probs = [(rows(g, m, k), rows(g, k, n), torch.zeros((m, -(-n // al) * al), device="cuda", dtype=dtype)[:, :n])
+             for m, n, k in shapes]
+    plan = cc.grouped(probs, precision=precision, slices=slices)
+    ws_max = max(cc.workspace_size(cc.make_desc(A, B, Cm, precision=precision, slices=slices)) for A, B, Cm in probs)
+    ws = torch.empty(max(ws_max, 256), dtype=torch.uint8, device="cuda")
+
+    def separate(stream):
+        for A, B, Cm in probs:
+            cc.gemm(A, B, Cm, precision=precision, slices=slices, workspace=ws, stream=stream)
+
+    plan()
+    n0 = cc.launch_count()
+    separate(None)
+    torch.cuda.synchronize()
+    launches_separate = cc.launch_count() - n0
+    s = torch.cuda.Stream()
+    g1, g2 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g1, stream=s):
+            plan(stream=s)
+        with torch.cuda.graph(g2, stream=s):
+            separate(s)
+
+    def timed(graph):
+        for _ in range(warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    t_grp, t_sep = timed(g1), timed(g2)
+    del g1, g2
+    plan.close()
+    return {"problems": len(shapes), "gflop": flop / 1e9, "grouped_ms": t_grp, "separate_ms": t_sep,
+            "tflops": flop / (t_grp * 1e-3) / 1e12, "separate_tflops": flop / (t_sep * 1e-3) / 1e12,
+            "speedup_vs_separate": t_sep / t_grp, "launches_grouped": 2 if precision != "ozaki" else 3,
+            "launches_separate": launches_separate,
+            "shapes": "M,N log-uniform [64,2048], K log-uniform [64,8192], seed %d" % seed}
 
 
 # -------------------------------------------------------------- CPU legs
@@ -313,6 +384,8 @@ def main():
     ap.add_argument("--size", type=int, default=8192)
     ap.add_argument("--ref-rows", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / error leg")
+    ap.add_argument("--only", default="", help="comma-separated subset of paths (profiling runs): "
+                    "bf16x3,bf16x6,native_f32,ozaki,native_f64,grouped_bf16x3,grouped_ozaki")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -335,11 +408,17 @@ def main():
     B64 = make_inputs(n, 4 + 10 * rank, torch.float64)
     C64 = torch.zeros((n, n), dtype=torch.float64, device="cuda")
 
-    paths = [("bf16x3", A32, B32, C32, 0), ("native_f32", A32, B32, C32, 0), ("ozaki", A64, B64, C64, OZAKI_SLICES),
-             ("native_f64", A64, B64, C64, 0)]
+    paths = [("bf16x3", A32, B32, C32, 0), ("bf16x6", A32, B32, C32, 0), ("native_f32", A32, B32, C32, 0),
+             ("ozaki", A64, B64, C64, OZAKI_SLICES), ("native_f64", A64, B64, C64, 0)]
+    if args.only:
+        keep = set(args.only.split(","))
+        paths = [p for p in paths if p[0] in keep]
     flop = 2.0 * n * n * n
     results, outs = {}, {}
-    clocks = None
+    # Clocks are sampled across all timed regions of this run (the headline
+    # region alone is tens of milliseconds, shorter than the sampling period).
+    sampler = ClockSampler(local)
+    sampler.start()
     for name, A, B, Cm, slices in paths:
         prec = "native" if name.startswith("native") else name
         d = cc.make_desc(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices)
@@ -351,14 +430,7 @@ def main():
                 results[name] = {"available": False}
                 continue
             raise
-        sampler = ClockSampler(local) if name == "bf16x3" or (clocks is None and name == "native_f32") else None
-        if sampler:
-            sampler.start()
         ms, kern_ms, launches = time_path(cc, A, B, Cm, prec, slices, args.steps, args.warmup, world, ws)
-        if sampler:
-            c = sampler.stop()
-            if name == "bf16x3" or clocks is None:
-                clocks = c
         ms = max_over_ranks(ms, world)
         tf = flop / (ms * 1e-3) / 1e12
         if name == "native_f32":
@@ -367,6 +439,8 @@ def main():
             peak, peak_name = sms * 64 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12, "FP64 (SMs x 64 x 2 x max clock)"
         elif name == "bf16x3":
             peak, peak_name = pk["bf16"] / 3, "measured bf16 dense / 3 products"
+        elif name == "bf16x6":
+            peak, peak_name = pk["bf16"] / 6, "measured bf16 dense / 6 products"
         else:
             peak = 2 * pk["bf16"] / (slices * (slices + 1) / 2)
             peak_name = "INT8 dense (2 x measured bf16) / %d slice products" % (slices * (slices + 1) // 2)
@@ -375,16 +449,29 @@ def main():
                          launches / args.steps, "workspace_bytes": (ws.numel() if ws is not None else 0)}
         outs[name] = Cm.cpu().numpy().copy() if rank == 0 and not args.no_cpu else None
 
-    head = "bf16x3" if results.get("bf16x3", {}).get("available") else "native_f32"
+    for gname, gprec, gdt, gsl in (("grouped_bf16x3", "bf16x3", torch.float32, 0),
+                                   ("grouped_ozaki", "ozaki", torch.float64, OZAKI_SLICES)):
+        if not args.only or gname in args.only.split(","):
+            results[gname] = grouped_bench(cc, gprec, gdt, gsl, max(3, args.steps), args.warmup, seed=5 + 10 * rank)
+    avail = [p for p in paths if results.get(p[0], {}).get("available")]
+    if not avail:  # a profiling run of the grouped launches only
+        clocks = sampler.stop()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "results": results, "clocks": clocks}), flush=True)
+        return 0
+    head_path = next((p for p in avail if p[0] == "bf16x3"), avail[0])
+    head, hA, hB, hC, hslices = head_path
+    hprec = "native" if head.startswith("native") else head
     hr = results[head]
-    A_h = A32.cpu().pin_memory()
-    B_h = B32.cpu().pin_memory()
-    C_h = torch.empty((n, n), dtype=torch.float32).pin_memory()
-    d = cc.make_desc(A32, B32, C32, precision=("bf16x3" if head == "bf16x3" else "native"))
+    A_h = hA.cpu().pin_memory()
+    B_h = hB.cpu().pin_memory()
+    C_h = torch.empty_like(hC, device="cpu").pin_memory()
+    d = cc.make_desc(hA, hB, hC, precision=hprec, slices=hslices)
     ws = cc.alloc_workspace(d)
-    e2e_ms = e2e_path(cc, A_h, B_h, C_h, A32, B32, C32, "bf16x3" if head == "bf16x3" else "native", 0,
-                      max(3, args.steps // 2), 2, ws)
+    e2e_ms = e2e_path(cc, A_h, B_h, C_h, hA, hB, hC, hprec, hslices, max(3, args.steps // 2), 2, ws)
     e2e_ms = max_over_ranks(e2e_ms, world)
+    clocks = sampler.stop()
+    es = hC.element_size()
 
     cpu, errs = (None, {})
     if rank == 0 and not args.no_cpu:
@@ -395,20 +482,22 @@ def main():
     # roofline of the headline's main kernel (useful flops / kernel time)
     kern_ms = hr.get("kernel_ms") or hr["ms"]
     achieved = flop / (kern_ms * 1e-3) / 1e12
-    roof = {"bound": "tensor" if head == "bf16x3" else "fp32-simt", "achieved": achieved, "peak": hr["peak_tflops"],
-            "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"], "traffic": None,
+    roof = {"bound": "tensor" if not head.startswith("native") else "simt", "achieved": achieved,
+            "peak": hr["peak_tflops"], "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"], "traffic": None,
             "peak_source": pk["source"] + ": " + hr["peak"], "kernel_ms": kern_ms}
+    dtypes = {"bf16x3": "bf16x3->f32", "bf16x6": "bf16x6->f32", "native_f32": "f32", "ozaki": "i8x%d->f64" % hslices,
+              "native_f64": "f64"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": hr["tflops"] * world, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16x3->f32" if head == "bf16x3" else "f32", "data": "synthetic",
-            "config": {"workload": "SGEMM %s %d^3, alpha=1 beta=0, U[-1,1]" % (head, n), "m": n, "n": n, "k": n,
+            "vs_baseline": None, "dtype": dtypes[head], "data": "synthetic",
+            "config": {"workload": "GEMM %s %d^3, alpha=1 beta=0, U[-1,1]" % (head, n), "m": n, "n": n, "k": n,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
-                       "l2": "inputs larger than L2 (%d MB per FP32 operand), no flush" % (n * n * 4 >> 20)},
+                       "l2": "inputs larger than L2 (%d MB per operand), no flush" % (n * n * es >> 20)},
             "e2e": {"value": flop / (e2e_ms * 1e-3) / 1e12 * world, "unit": "TFLOP/s",
-                    "h2d_bytes_per_step": 2 * n * n * 4, "d2h_bytes_per_step": n * n * 4},
+                    "h2d_bytes_per_step": 2 * n * n * es, "d2h_bytes_per_step": n * n * es},
             "gpu_launches": int(hr["launches_per_step"] * args.steps),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "results": results,
         }

@@ -224,5 +224,13 @@ def profile_stop():
     return ms.value, n.value
 
 
+def grouped(problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0):
+    """Plan a grouped launch over [(A, B, C), ...] device tensors; call the
+    returned object to enqueue it (two or three kernels, graph-capturable)."""
+    from ._ext import GroupedPlan
+
+    return GroupedPlan(problems, precision, alpha, beta, epilogue, slices)
+
+
 def set_wait_timeout_ns(ns):
     check(lib().cucosma_set_wait_timeout_ns(int(ns)), "cucosma_set_wait_timeout_ns")

@@ -1,16 +1,80 @@
-"""ctypes bindings of the optional entry points (grouped GEMM, sigmoid
-forward/backward, tuner).  Each binding is attached only if the symbol is
-exported by the loaded libcucosma.so."""
+"""ctypes bindings of the grouped-GEMM entry points (include/cucosma.h) and
+a small Python mirror used by the tests and bench.py."""
 from __future__ import annotations
 
 import ctypes as C
 
 
+class Problem(C.Structure):
+    """Mirror of cucosma_gemm_problem."""
+
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("k", C.c_int64), ("lda", C.c_int64), ("ldb", C.c_int64),
+                ("ldc", C.c_int64), ("A", C.c_void_p), ("B", C.c_void_p), ("C", C.c_void_p)]
+
+
 def bind(L):
+    from . import GemmDesc
+
     vp, sz = C.c_void_p, C.c_size_t
-    table = {}
+    P = C.POINTER(Problem)
+    table = {
+        "cucosma_grouped_workspace_size": ([C.POINTER(GemmDesc), P, C.c_int, C.POINTER(sz)], C.c_int),
+        "cucosma_grouped_plan_create": ([C.POINTER(GemmDesc), P, C.c_int, vp, sz, C.POINTER(vp)], C.c_int),
+        "cucosma_gemm_grouped": ([vp, vp], C.c_int),
+        "cucosma_grouped_plan_destroy": ([vp], C.c_int),
+    }
     for name, (argtypes, restype) in table.items():
         f = getattr(L, name, None)
         if f is not None:
             f.argtypes = argtypes
             f.restype = restype
+
+
+class GroupedPlan:
+    """A grouped launch bound to device tensors: problems is a list of
+    (A, B, C) row-major device tensors sharing dtype; the plan keeps them and
+    its workspace alive.  __call__ enqueues the launch on the current stream."""
+
+    def __init__(self, problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0):
+        import torch
+
+        from . import EPILOGUES, PRECISIONS, GemmDesc, _dtype_code, _ld, check, lib
+
+        L = lib()
+        self.problems = list(problems)
+        arr = (Problem * len(self.problems))()
+        for i, (A, B, Cm) in enumerate(self.problems):
+            arr[i] = Problem(A.shape[0], B.shape[1], A.shape[1], _ld(A), _ld(B), _ld(Cm), A.data_ptr(), B.data_ptr(),
+                             Cm.data_ptr())
+        d = GemmDesc()
+        L.cucosma_gemm_desc_init(C.byref(d))
+        d.dtype = _dtype_code(self.problems[0][2])
+        d.precision = PRECISIONS[precision]
+        d.epilogue = EPILOGUES[epilogue]
+        d.alpha, d.beta, d.slices = float(alpha), float(beta), int(slices)
+        n = C.c_size_t(0)
+        check(L.cucosma_grouped_workspace_size(C.byref(d), arr, len(self.problems), C.byref(n)),
+              "cucosma_grouped_workspace_size")
+        self.workspace = torch.empty(max(n.value, 256), dtype=torch.uint8, device=self.problems[0][2].device)
+        h = C.c_void_p()
+        check(L.cucosma_grouped_plan_create(C.byref(d), arr, len(self.problems), self.workspace.data_ptr(),
+                                            self.workspace.numel(), C.byref(h)), "cucosma_grouped_plan_create")
+        self.handle = h
+        self._arr = arr
+        self._lib = L
+
+    def __call__(self, stream=None):
+        from . import _stream_handle, check
+
+        check(self._lib.cucosma_gemm_grouped(self.handle, _stream_handle(stream)), "cucosma_gemm_grouped")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.cucosma_grouped_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

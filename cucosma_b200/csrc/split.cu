@@ -16,89 +16,88 @@
 #include <cuda_bf16.h>
 
 #include "split.cuh"
+#include "split_device.cuh"
 
 namespace cucosma {
 
 // ------------------------------------------------------------------ BF16
-__device__ __forceinline__ void split_bf16_value(float x, int nterms, __nv_bfloat16 (&t)[3]) {
-  float r = x;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    if (i < nterms) {
-      t[i] = __float2bfloat16_rn(r);
-      r = r - __bfloat162float(t[i]);
-    }
-  }
-}
-
 // A: rows x cols (ld elements) -> planes [nterms][rows][kpad], same layout.
-// Each thread converts 4 consecutive columns.
+// Rows stride over grid.y, 4-column groups over grid.x (no 64-bit division
+// per element); each thread converts 4 consecutive columns (one 16-byte
+// load, one 8-byte store per plane).  Columns cols..kpad-1 are written as 0.
 __global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
                                        int nterms, __nv_bfloat16* __restrict__ out) {
-  const int64_t c4 = ceil_div(cols, 4);
-  const int64_t total = (int64_t)rows * c4;
+  const int nc4 = (int)(kpad / 4);
   const int64_t plane = (int64_t)rows * kpad;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = idx / c4;
-    const int c = (int)(idx - r * c4) * 4;
-    const float* src = A + r * lda + c;
-    float v[4];
-    if (c + 4 <= cols) {
-      const float4 q = *reinterpret_cast<const float4*>(src);
-      v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
-    } else {
+  for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+    const float* srow = A + (int64_t)r * lda;
+    __nv_bfloat16* drow = out + (int64_t)r * kpad;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nc4; g += gridDim.x * blockDim.x) {
+      const int c = g * 4;
+      float v[4];
+      if (c + 4 <= cols) {
+        const float4 q = *reinterpret_cast<const float4*>(srow + c);
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+      } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) v[e] = c + e < cols ? src[e] : 0.f;
-    }
-    __nv_bfloat16 t[4][3];
+        for (int e = 0; e < 4; ++e) v[e] = c + e < cols ? srow[c + e] : 0.f;
+      }
+      __nv_bfloat16 t[4][3];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) split_bf16_value(v[e], nterms, t[e]);
-    for (int i = 0; i < nterms; ++i) {
-      __nv_bfloat16* dst = out + i * plane + r * kpad + c;
-      if (c + 4 <= kpad) {
-        // kpad is a multiple of 8: an aligned 8-byte store
-        __nv_bfloat162 lo = __halves2bfloat162(t[0][i], t[1][i]);
-        __nv_bfloat162 hi = __halves2bfloat162(t[2][i], t[3][i]);
+      for (int e = 0; e < 4; ++e) split_bf16_value(v[e], nterms, t[e]);
+      for (int i = 0; i < nterms; ++i) {
         uint2 pk;
-        pk.x = *reinterpret_cast<uint32_t*>(&lo);
-        pk.y = *reinterpret_cast<uint32_t*>(&hi);
-        *reinterpret_cast<uint2*>(dst) = pk;
+        pk.x = pack_bf16x2(t[0][i], t[1][i]);
+        pk.y = pack_bf16x2(t[2][i], t[3][i]);
+        *reinterpret_cast<uint2*>(drow + i * plane + c) = pk;  // kpad % 8 == 0: 8-byte aligned
       }
     }
   }
 }
 
 // B: K x N (ld elements) -> planes [nterms][N][kpad] (transposed), through a
-// 32 x 32 shared-memory tile.  Block = 32 x 8 threads.
+// 64 (k) x 64 (n) shared-memory tile; block 32 x 8.  Loads are 256-byte
+// rows of B (float2 per lane); each lane stores two consecutive k of one
+// output row as a 4-byte pair, so a warp writes 128 contiguous bytes per
+// plane.
 __global__ void split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
                                        int nterms, __nv_bfloat16* __restrict__ out) {
-  __shared__ float tile[32][33];
-  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
+  __shared__ float tile[64][65];
+  const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
   const int64_t plane = (int64_t)ncols * kpad;
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int k = k0 + i, n = n0 + threadIdx.x;
-    tile[i][threadIdx.x] = (k < krows && n < ncols) ? B[(int64_t)k * ldb + n] : 0.f;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+  for (int i = ty; i < 64; i += 8) {
+    const int k = k0 + i, n = n0 + 2 * tx;
+    const float* src = B + (int64_t)k * ldb + n;
+    float2 v = make_float2(0.f, 0.f);
+    if (k < krows) {
+      if (n + 1 < ncols) {
+        v = *reinterpret_cast<const float2*>(src);  // n even, ldb % 4 == 0: 8-byte aligned
+      } else if (n < ncols) {
+        v.x = src[0];
+      }
+    }
+    tile[i][2 * tx] = v.x;
+    tile[i][2 * tx + 1] = v.y;
   }
   __syncthreads();
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int n = n0 + i, k = k0 + threadIdx.x;
-    if (n < ncols && k < kpad) {
-      __nv_bfloat16 t[3];
-      split_bf16_value(tile[threadIdx.x][i], nterms, t);
-      for (int j = 0; j < nterms; ++j) out[j * plane + (int64_t)n * kpad + k] = t[j];
+  const int k = k0 + 2 * tx;
+#pragma unroll 2
+  for (int i = ty; i < 64; i += 8) {
+    const int n = n0 + i;
+    if (n < ncols && k < kpad) {  // kpad even, so k + 1 < kpad as well
+      __nv_bfloat16 t0[3], t1[3];
+      split_bf16_value(tile[2 * tx][i], nterms, t0);
+      split_bf16_value(tile[2 * tx + 1][i], nterms, t1);
+      __nv_bfloat16* dst = out + (int64_t)n * kpad + k;
+      for (int j = 0; j < nterms; ++j) *reinterpret_cast<uint32_t*>(dst + j * plane) = pack_bf16x2(t0[j], t1[j]);
     }
   }
 }
 
 // ----------------------------------------------------------------- Ozaki
 // frexp-style exponent of the largest magnitude: |x| < 2^e for all x.
-__device__ __forceinline__ int exp_of(double amax) {
-  if (amax == 0.0) return 0;
-  int e;
-  frexp(amax, &e);
-  return e;
-}
 
 // One warp per row of A.
 __global__ void ozaki_row_exp_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols,
@@ -131,27 +130,6 @@ __global__ void ozaki_col_exp_kernel(const double* __restrict__ B, int64_t ldb, 
   }
 }
 
-template <int S>
-__device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
-  double r = ldexp(v, -e);
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    r = r * 128.0;
-    const double w = trunc(r);
-    q[t] = (int8_t)(int)w;
-    r = r - w;
-  }
-}
-
-// Packed slice layout shared by both operands: for row r (a row of A, or a
-// column of B), k-block kb = k / 32 and slice p, the 32 bytes of k-block kb
-// of slice p are at r * (kpad * S) + kb * (32 * S) + p * 32.  Four slices of
-// one k-block thus fill one 128-byte row, the span of the 128-byte swizzle
-// the tensor cores read, and one TMA box row is 128 contiguous bytes.
-template <int S>
-__device__ __forceinline__ int64_t packed_index(int64_t r, int k, int64_t kpad, int p) {
-  return r * (kpad * S) + (int64_t)(k >> 5) * (32 * S) + p * 32 + (k & 31);
-}
 
 // A rows -> packed slices; each thread slices 4 consecutive columns.
 template <int S>
@@ -212,11 +190,13 @@ static unsigned grid_for(int64_t work, int threads, int sms) {
 cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
                               bool transpose, int sms, cudaStream_t st) {
   if (!transpose) {
-    split_bf16_rows_kernel<<<grid_for((int64_t)rows * ceil_div(cols, 4), 256, sms), 256, 0, st>>>(
-        A, lda, rows, cols, kpad, nterms, static_cast<__nv_bfloat16*>(out));
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(ceil_div(kpad / 4, 256), 16));
+    const int64_t gy = std::max<int64_t>(1, std::min<int64_t>({(int64_t)rows, (int64_t)sms * 16 / gx, 65535}));
+    split_bf16_rows_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(A, lda, rows, cols, kpad, nterms,
+                                                                               static_cast<__nv_bfloat16*>(out));
   } else {
     // A is K x N here (krows = rows, ncols = cols); output N x kpad.
-    dim3 grid((unsigned)ceil_div(cols, 32), (unsigned)ceil_div(kpad, 32));
+    dim3 grid((unsigned)ceil_div(cols, 64), (unsigned)ceil_div(kpad, 64));
     split_bf16_cols_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, rows, cols, kpad, nterms,
                                                          static_cast<__nv_bfloat16*>(out));
   }

@@ -1,0 +1,59 @@
+// split_device.cuh -- per-element device helpers of the operand pre-passes,
+// shared by the single-problem (split.cu) and grouped (grouped.cu) kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+
+namespace cucosma {
+
+// x = t0 + t1 (+ t2) + residual: each term the round-to-nearest-even BF16 of
+// what is left; every subtraction is exact in FP32 (Sterbenz).
+__device__ __forceinline__ void split_bf16_value(float x, int nterms, __nv_bfloat16 (&t)[3]) {
+  float r = x;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i < nterms) {
+      t[i] = __float2bfloat16_rn(r);
+      r = r - __bfloat162float(t[i]);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  __nv_bfloat162 v = __halves2bfloat162(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// frexp-style exponent of the largest magnitude: |x| < 2^e for all x.
+__device__ __forceinline__ int exp_of(double amax) {
+  if (amax == 0.0) return 0;
+  int e;
+  frexp(amax, &e);
+  return e;
+}
+
+// Ozaki slices of one value scaled into (-1, 1): r <- r * 2^7, q = trunc(r),
+// r <- r - q; exact in FP64 (power-of-two scaling, integer part removal).
+template <int S>
+__device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
+  double r = ldexp(v, -e);
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    r = r * 128.0;
+    const double w = trunc(r);
+    q[t] = (int8_t)(int)w;
+    r = r - w;
+  }
+}
+
+// Packed slice layout shared by both operands: for row r (a row of A, or a
+// column of B), k-block kb = k / 32 and slice p, the 32 bytes of k-block kb
+// of slice p are at r * (kpad * S) + kb * (32 * S) + p * 32.  Four slices of
+// one k-block thus fill one 128-byte row, the span of the 128-byte swizzle
+// the tensor cores read, and one TMA box row is 128 contiguous bytes.
+template <int S>
+__device__ __forceinline__ int64_t packed_index(int64_t r, int k, int64_t kpad, int p) {
+  return r * (kpad * S) + (int64_t)(k >> 5) * (32 * S) + p * 32 + (k & 31);
+}
+
+}  // namespace cucosma

@@ -10,7 +10,27 @@ constexpr int kOzakiDefaultSlices = 8;
 
 namespace tc {
 
-constexpr int kThreads = 192;  // producer warp, MMA warp, 4 epilogue warps
+// One problem of a grouped launch, stored in the workspace.  The tensor maps
+// describe this problem's operand planes (they live in global memory; the
+// TMA unit reads them there).  Tiles of all problems are numbered
+// consecutively: this problem owns [tile_start, tile_start + tiles_m*tiles_n).
+struct alignas(64) GroupEntry {
+  CUtensorMap tmA, tmB;
+  void* C;
+  int64_t ldc;
+  const int32_t* ea;  // Ozaki exponents of this problem (null for BF16)
+  const int32_t* eb;
+  int m, n, k, kblocks;
+  int tiles_m, tiles_n, tile_start, pad0;
+  // operand pre-pass: sources, destination planes, first pre-pass block of
+  // this problem for the A rows / B tiles / exponent passes
+  const void* A;
+  const void* B;
+  int64_t lda, ldb, kpad;
+  void* planes_a;
+  void* planes_b;
+  int pre_a_start, pre_b_start, exp_a_start, exp_b_start;
+};
 
 struct TcParams {
   int m, n, k;
@@ -28,6 +48,28 @@ struct TcParams {
   const int32_t* ea;  // Ozaki row exponents of A
   const int32_t* eb;  // Ozaki column exponents of B
   WaitCtl ctl;
+  // Grouped launch: when ngroups > 0 the problems come from groups[] (all
+  // other per-problem fields above are ignored) and units = total_tiles.
+  const GroupEntry* groups;
+  int ngroups, total_tiles;
+};
+
+// Where a work unit's result goes (from TcParams, or from a GroupEntry).
+struct OutCtx {
+  int m, n, epilogue, partial;
+  double alpha, beta;
+  void* out;
+  int64_t ldo, ws_split_stride;
+  const int32_t* ea;
+  const int32_t* eb;
+};
+
+// A resolved work unit: operand descriptors, tile coordinates, K range.
+struct Unit {
+  const CUtensorMap* ta;
+  const CUtensorMap* tb;
+  int tm, tn, z, kb0, kb1;
+  int group;  // -1 when not grouped
 };
 
 }  // namespace tc

@@ -1,0 +1,626 @@
+// tc_kernel.cuh -- the tcgen05 kernel template, its epilogues and the
+// traits of every precision path (included by tc_gemm.cu and grouped.cu).
+//
+//
+// One persistent, warp-specialised kernel template serves both precision
+// forms that have no counterpart in the reference (which is FP32 SIMT only,
+// cuCOSMAV100.cuh:2505-2756):
+//
+//   BF16x3 / BF16x6 SGEMM   A = sum_i A_i, B = sum_j B_j (BF16 split planes);
+//                           C ~= sum over the kept (i, j) of A_i * B_j, all
+//                           products accumulated in one FP32 TMEM accumulator.
+//   Ozaki DGEMM (INT8)      A_p, B_q signed 7-bit slices; for every diagonal
+//                           d = p + q < s an exact INT32 TMEM accumulator
+//                           S_d = sum_{p+q=d} A_p * B_q; the epilogue
+//                           recombines sum_d S_d 2^(-7(d+2)) in FP64 (d
+//                           descending) and rescales by 2^(e_row + e_col).
+//
+// Roles (192 threads): warp 0 lane 0 streams the slice planes of A and B
+// with 3-D TMA loads (all planes of one k-block in one box) into a
+// multi-stage shared-memory ring; warp 1 allocates TMEM and one lane issues
+// tcgen05.mma (A and B from shared memory, K-major, swizzled) and commits to
+// mbarriers; warps 2-5 drain the accumulators (tcgen05.ld), apply
+// alpha/beta and the fused epilogue and store through a shared-memory
+// transpose for coalesced rows.  Accumulators are double-buffered in TMEM
+// when they fit, so the epilogue of one tile overlaps the next tile's MMAs.
+// Work units (tile x K split) are distributed round-robin over a persistent
+// grid with a banded raster (the reference's block swizzle,
+// cuCOSMAV100.cuh:2586-2603, generalised).  Split-K writes raw partials to
+// the workspace and a separate kernel reduces them in split order.
+//
+// Every mbarrier wait is bounded (ptx.cuh); on expiry the roles leave their
+// loops, drain what they issued, and TMEM is released before exit.
+#pragma once
+#include <cuda_bf16.h>
+
+#include <utility>
+
+#include "api_internal.cuh"
+#include "tc_gemm.cuh"
+
+namespace cucosma {
+namespace tc {
+
+// Shared-memory matrix descriptor, K-major operand written by TMA with a
+// swizzle span of SWZ bytes per row: start >> 4 at [0,14), leading byte
+// offset (unused for swizzled K-major) at [16,30), stride byte offset
+// (8 rows x SWZ) >> 4 at [32,46), version 1 at [46,48), layout type at
+// [61,64): 2 = 128B, 4 = 64B, 6 = 32B swizzle.
+template <int SWZ>
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  constexpr uint64_t layout = SWZ == 128 ? 2 : (SWZ == 64 ? 4 : 6);
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)((8 * SWZ) >> 4) << 32) |
+         ((uint64_t)1 << 46) | (layout << 61);
+}
+
+__device__ __forceinline__ void unit_coords(int unit, int tiles, int tiles_m, int tiles_n, int band, int& z, int& tm,
+                                            int& tn) {
+  z = unit / tiles;
+  const int t = unit - z * tiles;
+  const int per_band = band * tiles_n;
+  const int b = t / per_band;
+  const int w = t - b * per_band;
+  const int rows = min(band, tiles_m - b * band);
+  tm = b * band + w % rows;
+  tn = w / rows;
+}
+
+// Unit -> (operand descriptors, tile, K range).  Single problem: banded
+// raster over tiles x K splits.  Grouped: the problem owning the unit is
+// found by binary search over the tile_start column of the problem table;
+// its tiles are visited down M first, then across N.
+__device__ __forceinline__ void resolve_unit(const TcParams& p, const CUtensorMap* tmA, const CUtensorMap* tmB,
+                                             int unit, Unit& u) {
+  if (p.ngroups == 0) {
+    unit_coords(unit, p.tiles_m * p.tiles_n, p.tiles_m, p.tiles_n, p.band, u.z, u.tm, u.tn);
+    u.kb0 = u.z * p.kb_per_split;
+    u.kb1 = min(p.kblocks, u.kb0 + p.kb_per_split);
+    u.ta = tmA;
+    u.tb = tmB;
+    u.group = -1;
+  } else {
+    int lo = 0, hi = p.ngroups - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (p.groups[mid].tile_start <= unit)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const GroupEntry& e = p.groups[lo];
+    const int local = unit - e.tile_start;
+    u.tm = local % e.tiles_m;
+    u.tn = local / e.tiles_m;
+    u.z = 0;
+    u.kb0 = 0;
+    u.kb1 = e.kblocks;
+    u.ta = &e.tmA;
+    u.tb = &e.tmB;
+    u.group = lo;
+  }
+}
+
+__device__ __forceinline__ OutCtx out_ctx(const TcParams& p, const Unit& u) {
+  OutCtx o;
+  o.epilogue = p.epilogue;
+  o.alpha = p.alpha;
+  o.beta = p.beta;
+  if (u.group < 0) {
+    o.m = p.m;
+    o.n = p.n;
+    o.partial = p.partial;
+    o.out = p.out;
+    o.ldo = p.ldo;
+    o.ws_split_stride = p.ws_split_stride;
+    o.ea = p.ea;
+    o.eb = p.eb;
+  } else {
+    const GroupEntry& e = p.groups[u.group];
+    o.m = e.m;
+    o.n = e.n;
+    o.partial = 0;
+    o.out = e.C;
+    o.ldo = e.ldc;
+    o.ws_split_stride = 0;
+    o.ea = e.ea;
+    o.eb = e.eb;
+  }
+  return o;
+}
+
+// Issues the MMAs of term T for one stage.  Descriptor start addresses
+// advance by compile-time offsets (>> 4, no carry out of the 14-bit field
+// since every operand lies inside shared memory).
+template <class Tr, int T>
+__device__ __forceinline__ void issue_term(uint64_t ad0, uint64_t bd0, uint32_t acc0, bool not_first_kb) {
+  constexpr int KSTEPS = Tr::KSTEPS;
+  constexpr int PA = Tr::kTerms.a[T], PB = Tr::kTerms.b[T], D = Tr::kTerms.d[T];
+  constexpr bool FIRST = Tr::kTerms.first[T];
+  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, Tr::BN) : idesc_bf16_f32(128, Tr::BN);
+#pragma unroll
+  for (int kk = 0; kk < KSTEPS; ++kk) {
+    const uint64_t ad = ad0 + (uint64_t)(Tr::a_off(PA, kk) >> 4);
+    const uint64_t bd = bd0 + (uint64_t)(Tr::b_off(PB, kk) >> 4);
+    const bool acc = (FIRST && kk == 0) ? not_first_kb : true;
+    if constexpr (Tr::kInt8)
+      mma_i8(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+    else
+      mma_bf16(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+  }
+}
+template <class Tr, int... Ts>
+__device__ __forceinline__ void issue_terms(std::integer_sequence<int, Ts...>, uint64_t ad0, uint64_t bd0, uint32_t acc0,
+                                            bool not_first_kb) {
+  (issue_term<Tr, Ts>(ad0, bd0, acc0, not_first_kb), ...);
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(Tr::THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+  constexpr int BN = Tr::BN, SWZ = Tr::SWZ, NA = Tr::NA, NB = Tr::NB, NACC = Tr::NACC, ST = Tr::STAGES;
+  constexpr int A_REGION = Tr::A_REGION;
+  constexpr int STAGE_BYTES = Tr::STAGE_BYTES;
+  constexpr int NBUF = Tr::NBUF;
+  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, BN) : idesc_bf16_f32(128, BN);
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* stages = smem;
+  uint8_t* staging = smem + ST * STAGE_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + Tr::STAGING_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + ST;
+  uint64_t* tfull = bars + 2 * ST;
+  uint64_t* tempty = tfull + 4;
+  uint64_t* drain = tempty + 4;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  static_assert(NBUF <= 4, "accumulator buffers");
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int units = p.ngroups > 0 ? p.total_tiles : p.tiles_m * p.tiles_n * p.splits;
+  // K-blocks per accumulator chunk: with promotion the tensor cores
+  // accumulate CHUNK k-blocks in TMEM and the epilogue warps add each chunk
+  // into FP32 registers (round to nearest); otherwise one chunk per unit.
+  const int chunk = Tr::PROMOTE ? Tr::CHUNK : (1 << 30);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 4; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], Tr::EPI_WARPS);
+    }
+    mbar_init(drain, 1);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_holder, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    if (lane == 0) {
+      if (p.ngroups == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+      }
+      int it = 0;  // global k-block counter (ring position)
+      bool ok = true;
+      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+        Unit u;
+        resolve_unit(p, &tmA, &tmB, unit, u);
+        const int tm = u.tm, tn = u.tn;
+        for (int kb = u.kb0; kb < u.kb1; ++kb, ++it) {
+          const int s = it % ST;
+          if (!mbar_wait(&empty[s], ((it / ST) & 1) ^ 1, kErrTimeoutEmpty, p.ctl)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = stages + s * STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+          if constexpr (Tr::PACKED) {
+            // boxes of [rows][128 B]: slices 4j..4j+3 of k-block kb
+#pragma unroll
+            for (int j = 0; j < Tr::TILES_A; ++j) tma_load_3d(st + j * Tr::A_TILE, u.ta, j * 128, kb, tm * 128, &full[s]);
+#pragma unroll
+            for (int j = 0; j < Tr::TILES_B; ++j)
+              tma_load_3d(st + A_REGION + j * Tr::B_TILE, u.tb, j * 128, kb, tn * BN, &full[s]);
+          } else {
+            // one box of [planes][rows][BK] per operand
+            tma_load_3d(st, u.ta, kb * Tr::BK, tm * 128, 0, &full[s]);
+            tma_load_3d(st + A_REGION, u.tb, kb * Tr::BK, tn * BN, 0, &full[s]);
+          }
+        }
+      }
+      if (!ok)  // drain loads that may still be in flight (bounded)
+        for (int j = max(0, it - ST); j < it; ++j) mbar_wait(&full[j % ST], (j / ST) & 1, kErrTimeoutDrain, p.ctl);
+    }
+  } else if (warp == 1) {
+    // -------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int it = 0, ci = 0;
+      bool ok = true;
+      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+        Unit u;
+        resolve_unit(p, &tmA, &tmB, unit, u);
+        const int kb1 = u.kb1;
+        for (int cs = u.kb0; cs < kb1 && ok; cs += chunk, ++ci) {
+          const int ce = min(kb1, cs + chunk);
+          const int buf = ci % NBUF;
+          if (!mbar_wait(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t acc0 = tmem_base + (uint32_t)(buf * NACC * BN);
+          for (int kb = cs; kb < ce; ++kb, ++it) {
+            const int s = it % ST;
+            if (!mbar_wait(&full[s], (it / ST) & 1, kErrTimeoutFull, p.ctl)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
+            const uint64_t ad0 = sdesc<SWZ>(a_base);
+            const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
+            issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != cs);
+            mma_commit(&empty[s]);  // stage free once these MMAs have read it
+          }
+          if (!ok) break;
+          mma_commit(&tfull[buf]);  // accumulator ready once every MMA above completes
+        }
+      }
+      if (!ok) {
+        mma_commit(drain);  // wait (bounded) for every MMA issued so far
+        mbar_wait(drain, 0, kErrTimeoutDrain, p.ctl);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    // Epilogue warp ew: TMEM lane quadrant warp % 4 (the only lanes a warp may
+    // access) and, with 8 epilogue warps, one half of the tile's columns.
+    const int q = warp & 3;
+    constexpr int W = Tr::COLS_PER_EW;
+    const int colsub = ((warp - 2) / 4) * W;
+    const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
+    uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
+    int ci = 0;
+    bool ok = true;
+    for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+      Unit u;
+      resolve_unit(p, &tmA, &tmB, unit, u);
+      const OutCtx o = out_ctx(p, u);
+      const int z = u.z;
+      const int row0 = u.tm * 128 + 32 * q;
+      const int col0 = u.tn * BN;
+      if constexpr (Tr::PROMOTE) {
+        float master[W];
+#pragma unroll
+        for (int j = 0; j < W; ++j) master[j] = 0.f;
+        for (int cs = u.kb0; cs < u.kb1; cs += chunk, ++ci) {
+          const int buf = ci % NBUF;
+          ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
+          if (!ok) break;
+          tc_fence_after();
+          Tr::accumulate(lane_base + (uint32_t)(buf * NACC * BN + colsub), master);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        if (!ok) break;
+        Tr::finish(o, master, stg, lane, row0, col0 + colsub, z);
+      } else {
+        const int buf = ci % NBUF;
+        ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
+        if (!ok) break;
+        tc_fence_after();
+        Tr::epilogue(o, lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+        ++ci;
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncwarp();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// ------------------------------------------------------------ epilogues
+// FP32 result (BF16 split paths).  Each warp owns 32 rows; chunks of 32
+// columns go TMEM -> registers -> padded shared tile -> coalesced rows.
+struct EpiF32 {
+  static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
+
+  // Stores the 32 x 32 block staged in stg (row r of the warp's rows in
+  // stg[r * 33 + ...]) at columns col0 + c0 + [0, 32): coalesced rows.
+  static __device__ __forceinline__ void store32(const OutCtx& p, const float* stg, int lane, int row0, int col,
+                                                 int z) {
+    if (col >= p.n) return;
+    if (p.partial) {
+      float* w = reinterpret_cast<float*>(p.out) + (int64_t)z * p.ws_split_stride + col;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = row0 + r;
+        if (row < p.m) w[(int64_t)row * p.ldo] = stg[r * 33 + lane];
+      }
+    } else {
+      const float alpha = (float)p.alpha, beta = (float)p.beta;
+      float* o = reinterpret_cast<float*>(p.out) + col;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = row0 + r;
+        if (row < p.m) {
+          float* po = o + (int64_t)row * p.ldo;
+          *po = apply_epi(combine(stg[r * 33 + lane], alpha, beta, po), p.epilogue);
+        }
+      }
+    }
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
+                                             int col0, int z) {
+    float* stg = reinterpret_cast<float*>(stg_raw);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t v0[16], v1[16];
+      tmem_ld16(tacc + c0, v0);
+      tmem_ld16(tacc + c0 + 16, v1);
+      tmem_ld_wait();
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        stg[lane * 33 + j] = __uint_as_float(v0[j]);
+        stg[lane * 33 + 16 + j] = __uint_as_float(v1[j]);
+      }
+      __syncwarp();
+      store32(p, stg, lane, row0, col0 + c0 + lane, z);
+      __syncwarp();
+    }
+  }
+
+  // Promotion: add one chunk's TMEM accumulators (this thread's row, BN
+  // columns each; the correction products' accumulator NACC-1 first, the
+  // main product's accumulator 0 last) into the FP32 register accumulator,
+  // rounding to nearest.
+  // W columns of this warp (from tacc); accumulators STRIDE columns apart.
+  template <int W, int STRIDE, int NACC>
+  static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[W]) {
+#pragma unroll
+    for (int d = NACC - 1; d >= 0; --d) {
+#pragma unroll
+      for (int c0 = 0; c0 < W; c0 += 32) {
+        uint32_t v0[16], v1[16];
+        tmem_ld16(tacc + d * STRIDE + c0, v0);
+        tmem_ld16(tacc + d * STRIDE + c0 + 16, v1);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          master[c0 + j] = __fadd_rn(master[c0 + j], __uint_as_float(v0[j]));
+          master[c0 + 16 + j] = __fadd_rn(master[c0 + 16 + j], __uint_as_float(v1[j]));
+        }
+      }
+    }
+  }
+
+  template <int BN>
+  static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[BN], uint8_t* stg_raw,
+                                                int lane, int row0, int col0, int z) {
+    float* stg = reinterpret_cast<float*>(stg_raw);
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = master[c0 + j];
+      __syncwarp();
+      store32(p, stg, lane, row0, col0 + c0 + lane, z);
+      __syncwarp();
+    }
+  }
+};
+
+// FP64 result (Ozaki).  Chunks of 16 columns: part = sum_{d = S-1..0}
+// S_d * 2^(-7(d+2)) (FP64, d descending), then 2^(e_row + e_col) and
+// alpha/beta; or the raw part into the split-K workspace.
+template <int S>
+struct EpiOzaki {
+  static constexpr int STAGING_PER_WARP = 32 * 17 * 8;
+  template <int BN>
+  static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
+                                             int col0, int z) {
+    double* stg = reinterpret_cast<double*>(stg_raw);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      double part[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) part[j] = 0.0;
+#pragma unroll
+      for (int d = S - 1; d >= 0; --d) {
+        uint32_t v[16];
+        tmem_ld16(tacc + d * BN + c0, v);
+        tmem_ld_wait();
+        const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+        for (int j = 0; j < 16; ++j) part[j] = part[j] + (double)(int32_t)v[j] * w;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = part[j];
+      __syncwarp();
+      const int cl = lane & 15;
+      const int col = col0 + c0 + cl;
+      if (col < p.n) {
+        const int ecol = p.partial ? 0 : p.eb[col];
+#pragma unroll 4
+        for (int h = 0; h < 16; ++h) {
+          const int r = (lane >> 4) + 2 * h;
+          const int row = row0 + r;
+          if (row >= p.m) continue;
+          const double v = stg[r * 17 + cl];
+          if (p.partial) {
+            reinterpret_cast<double*>(p.out)[(int64_t)z * p.ws_split_stride + (int64_t)row * p.ldo + col] = v;
+          } else {
+            double* po = reinterpret_cast<double*>(p.out) + (int64_t)row * p.ldo + col;
+            const double r_ = ldexp(v, p.ea[row] + ecol);
+            const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * *po);
+            *po = apply_epi(o, p.epilogue);
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+};
+
+// ------------------------------------------------------------- traits
+constexpr int kSmemBudget = 227 * 1024;
+
+// Stage layout.  Unpacked (BF16 planes): one tile of rows x SWZ bytes per
+// plane, KSTEPS MMAs of 32 bytes of K each per plane pair.  Packed (Ozaki
+// INT8 slices): one stage is one 32-wide k-block; four slices share each
+// 128-byte swizzled row, so slice p sits in tile p / 4 at byte offset
+// (p % 4) * 32 -- selected like a K offset inside the swizzle atom.
+template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi, bool PROMOTE_ = false,
+          int CHUNK_ = 0, int EPI_WARPS_ = 4>
+struct TraitsBase {
+  static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
+  static constexpr bool kInt8 = INT8_;
+  static constexpr bool PROMOTE = PROMOTE_;
+  static constexpr int CHUNK = CHUNK_;
+  // 4 epilogue warps (one per TMEM lane quadrant) or 8 (each quadrant
+  // split into two column halves, so promoted register accumulators fit).
+  static constexpr int EPI_WARPS = EPI_WARPS_;
+  static constexpr int THREADS = (2 + EPI_WARPS) * 32;
+  static constexpr int COLS_PER_EW = BN / (EPI_WARPS / 4);
+  static_assert(EPI_WARPS == 4 || (EPI_WARPS == 8 && PROMOTE_), "8 epilogue warps only for promotion");
+  static constexpr bool PACKED = INT8_;
+  static constexpr int BK = PACKED ? 32 : SWZ / 2;  // K elements per stage
+  static constexpr int KSTEPS = PACKED ? 1 : SWZ / 32;
+  static constexpr int TILES_A = PACKED ? (NA + 3) / 4 : NA;  // TMA boxes per operand per stage
+  static constexpr int TILES_B = PACKED ? (NB + 3) / 4 : NB;
+  static constexpr int A_TILE = 128 * SWZ, B_TILE = BN * SWZ;
+  static constexpr int A_REGION = TILES_A * A_TILE;
+  static constexpr __host__ __device__ int a_off(int p, int kk) {
+    return PACKED ? (p / 4) * A_TILE + (p % 4) * 32 : p * A_TILE + kk * 32;
+  }
+  static constexpr __host__ __device__ int b_off(int q, int kk) {
+    return PACKED ? (q / 4) * B_TILE + (q % 4) * 32 : q * B_TILE + kk * 32;
+  }
+  static constexpr int NBUF =
+      PROMOTE ? (512 / (NACC * BN) > 4 ? 4 : 512 / (NACC * BN)) : ((2 * NACC * BN <= 512) ? 2 : 1);
+  static constexpr int STAGING_PER_WARP = Epi::STAGING_PER_WARP;
+  static constexpr int STAGING_BYTES = EPI_WARPS * STAGING_PER_WARP;
+  static constexpr int STAGE_BYTES = TILES_A * A_TILE + TILES_B * B_TILE;
+  static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
+  static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
+  static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
+  static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
+  static_assert(STAGES >= 2, "at least a double-buffered ring");
+  static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
+  static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
+  static_assert(!PROMOTE || (CHUNK > 0 && NBUF >= 2), "promotion needs chunk buffers");
+  static __device__ __forceinline__ void epilogue(const OutCtx& p, uint32_t tacc, uint8_t* stg, int lane, int row0,
+                                                  int col0, int z) {
+    Epi::template run<BN>(p, tacc, stg, lane, row0, col0, z);
+  }
+  static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[COLS_PER_EW]) {
+    if constexpr (PROMOTE) Epi::template accumulate<COLS_PER_EW, BN, NACC>(tacc, master);
+  }
+  static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[COLS_PER_EW], uint8_t* stg,
+                                                int lane, int row0, int col0, int z) {
+    if constexpr (PROMOTE) Epi::template finish<COLS_PER_EW>(p, master, stg, lane, row0, col0, z);
+  }
+};
+
+// K-blocks (32 wide) the tensor cores accumulate before the epilogue adds
+// the chunk into its FP32 registers.
+constexpr int kPromoteChunk = 4;
+
+// BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
+// Term tables: for term t, the A plane a[t], the B plane b[t], the
+// accumulator d[t], and whether t is the first term of the k-block order to
+// write accumulator d[t] (that MMA overwrites instead of accumulating on the
+// first k-block of a unit).  Built at compile time.
+template <int NT>
+struct TermTable {
+  int a[NT], b[NT], d[NT];
+  bool first[NT];
+};
+
+// BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
+// Default (tile id 0): 128 x 256 tiles, one TMEM accumulator promoted into
+// FP32 registers every kPromoteChunk k-blocks by 8 epilogue warps (two per
+// lane quadrant, 128 columns each): without promotion the truncating
+// accumulation grows its error linearly in K.  Tile id 1: the same tile
+// without promotion (whole K in TMEM).  Tile id 2: 128 x 128 tiles with
+// promotion and the correction products in their own accumulator.
+struct Bf16x3 : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
+};
+struct Bf16x3Wide : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
+};
+struct Bf16x3Promoted : TraitsBase<3, 128, 64, 2, 2, 2, false, EpiF32, true, kPromoteChunk> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {true, false, true}};
+};
+
+// BF16x6: 3-way split, the six products with i + j <= 2; the five
+// correction products accumulate in TMEM accumulator 1, the main product
+// hi*hi in accumulator 0, so the main accumulator is rounded only by its own
+// MMAs; both are promoted into FP32 registers every kPromoteChunk k-blocks.
+struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk> {
+  static constexpr TermTable<6> kTerms{
+      {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
+};
+
+// Ozaki with S slices: all pairs (p, q) with p + q < S, ordered by p then q;
+// accumulator d = p + q (the first writer of diagonal d is (0, d)); BN chosen
+// so that S accumulators fit in TMEM.
+template <int S>
+struct OzakiBN {
+  static constexpr int value = S <= 8 ? 64 : (S <= 10 ? 48 : 32);
+};
+template <int S>
+constexpr TermTable<S*(S + 1) / 2> ozaki_terms() {
+  TermTable<S*(S + 1) / 2> t{};
+  int i = 0;
+  for (int p = 0; p < S; ++p)
+    for (int q = 0; p + q < S; ++q) {
+      t.a[i] = p;
+      t.b[i] = q;
+      t.d[i] = p + q;
+      t.first[i] = p == 0;
+      ++i;
+    }
+  return t;
+}
+template <int S>
+struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, EpiOzaki<S>> {
+  static constexpr TermTable<S*(S + 1) / 2> kTerms = ozaki_terms<S>();
+};
+
+template <class Tr>
+static cudaError_t launch(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p, int grid, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tr::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  tc_gemm_kernel<Tr><<<grid, Tr::THREADS, Tr::SMEM, st>>>(a, b, p);
+  return cudaGetLastError();
+}
+
+}  // namespace tc
+}  // namespace cucosma

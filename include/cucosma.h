@@ -121,6 +121,38 @@ CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
                              double beta, double* C, int ldc, void* stream);
 
+/* ---------------------------------------------------------------- grouped
+ * Many independent GEMMs of uneven sizes in one persistent launch (no
+ * counterpart in the reference, whose sizes are compile-time macros: one
+ * build per shape).  Every problem shares the descriptor's dtype, precision
+ * (BF16X3, BF16X6 or OZAKI), slices, epilogue, alpha and beta; the m, n, k,
+ * ld* fields of the descriptor are ignored.  A plan binds the problems (their
+ * device pointers and sizes) to a caller workspace: plan creation encodes one
+ * pair of TMA descriptors per problem and uploads the problem table into the
+ * workspace (synchronous).  cucosma_gemm_grouped then enqueues exactly two
+ * kernels (BF16 paths: operand split, GEMM) or three (Ozaki: exponents,
+ * slices, GEMM), allocates nothing and copies nothing from the host, so it
+ * can be captured in a CUDA graph and replayed while the plan lives. */
+typedef struct cucosma_gemm_problem {
+  int64_t m, n, k;
+  int64_t lda, ldb, ldc;
+  const void* A;
+  const void* B;
+  void* C;
+} cucosma_gemm_problem;
+
+typedef struct cucosma_grouped_plan_st* cucosma_grouped_plan;
+
+CUCOSMA_API cucosma_status cucosma_grouped_workspace_size(const cucosma_gemm_desc* d,
+                                                          const cucosma_gemm_problem* problems, int count,
+                                                          size_t* bytes);
+CUCOSMA_API cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d,
+                                                       const cucosma_gemm_problem* problems, int count,
+                                                       void* workspace, size_t workspace_bytes,
+                                                       cucosma_grouped_plan* plan);
+CUCOSMA_API cucosma_status cucosma_gemm_grouped(cucosma_grouped_plan plan, void* stream);
+CUCOSMA_API cucosma_status cucosma_grouped_plan_destroy(cucosma_grouped_plan plan);
+
 /* Allocation-free FP32 split-K GEMM.  No counterpart in the reference (whose
  * split-K path cudaMallocs its workspace on every call).  For callers that
  * must not allocate device memory -- e.g. a plugin whose host framework owns
