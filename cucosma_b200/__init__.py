@@ -224,6 +224,26 @@ def profile_stop():
     return ms.value, n.value
 
 
+def gemm_backward(A, B, Y, dY, dA=None, dB=None, alpha=1.0, precision="bf16x3", epilogue="sigmoid", workspace=None,
+                  stream=None):
+    """Gradients of Y = epi(alpha*A@B + beta*C0): dA = G@B^T, dB = A^T@G with
+    G = alpha * dY * epi'(Z) (epi' from the saved Y).  Writes dA / dB in place."""
+    import torch
+
+    L = lib()
+    d = make_desc(A, B, Y, alpha, 0.0, precision=precision, epilogue=epilogue)
+    if workspace is None:
+        n = C.c_size_t(0)
+        check(L.cucosma_gemm_backward_workspace_size(C.byref(d), C.byref(n)), "cucosma_gemm_backward_workspace_size")
+        workspace = torch.empty(max(n.value, 256), dtype=torch.uint8, device=Y.device)
+    ws_n = workspace.numel() * workspace.element_size()
+    check(L.cucosma_gemm_backward(C.byref(d), A.data_ptr(), B.data_ptr(), Y.data_ptr(), _ld(Y), dY.data_ptr(), _ld(dY),
+                                  dA.data_ptr() if dA is not None else None, _ld(dA) if dA is not None else 0,
+                                  dB.data_ptr() if dB is not None else None, _ld(dB) if dB is not None else 0,
+                                  workspace.data_ptr(), ws_n, _stream_handle(stream)), "cucosma_gemm_backward")
+    return dA, dB
+
+
 def grouped(problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0):
     """Plan a grouped launch over [(A, B, C), ...] device tensors; call the
     returned object to enqueue it (two or three kernels, graph-capturable)."""

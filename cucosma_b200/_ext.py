@@ -22,6 +22,9 @@ def bind(L):
         "cucosma_grouped_plan_create": ([C.POINTER(GemmDesc), P, C.c_int, vp, sz, C.POINTER(vp)], C.c_int),
         "cucosma_gemm_grouped": ([vp, vp], C.c_int),
         "cucosma_grouped_plan_destroy": ([vp], C.c_int),
+        "cucosma_gemm_backward_workspace_size": ([C.POINTER(GemmDesc), C.POINTER(sz)], C.c_int),
+        "cucosma_gemm_backward": ([C.POINTER(GemmDesc), vp, vp, vp, C.c_int64, vp, C.c_int64, vp, C.c_int64, vp,
+                                   C.c_int64, vp, sz, vp], C.c_int),
     }
     for name, (argtypes, restype) in table.items():
         f = getattr(L, name, None)

@@ -42,6 +42,10 @@ cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, cons
 void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info);
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                        const DeviceInfo* di, cudaStream_t st);
+// BF16 paths only: planes_ready = true skips the split pre-pass (the caller
+// has written the operand planes at the plan's offsets in ws).
+cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
+                          const DeviceInfo* di, cudaStream_t st, bool planes_ready);
 
 void* managed_workspace(size_t bytes);
 

@@ -25,8 +25,10 @@ namespace cucosma {
 // Rows stride over grid.y, 4-column groups over grid.x (no 64-bit division
 // per element); each thread converts 4 consecutive columns (one 16-byte
 // load, one 8-byte store per plane).  Columns cols..kpad-1 are written as 0.
+template <int MODE>
 __global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
-                                       int nterms, __nv_bfloat16* __restrict__ out) {
+                                       int nterms, __nv_bfloat16* __restrict__ out, const float* __restrict__ Y,
+                                       int64_t ldy, float scale) {
   const int nc4 = (int)(kpad / 4);
   const int64_t plane = (int64_t)rows * kpad;
   for (int r = blockIdx.y; r < rows; r += gridDim.y) {
@@ -41,6 +43,19 @@ __global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda,
       } else {
 #pragma unroll
         for (int e = 0; e < 4; ++e) v[e] = c + e < cols ? srow[c + e] : 0.f;
+      }
+      if constexpr (MODE != kXformNone) {
+        const float* yrow = Y + (int64_t)r * ldy;
+        float y[4];
+        if (c + 4 <= cols) {
+          const float4 q = *reinterpret_cast<const float4*>(yrow + c);
+          y[0] = q.x, y[1] = q.y, y[2] = q.z, y[3] = q.w;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) y[e] = c + e < cols ? yrow[c + e] : 0.f;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[e] = xform<MODE>(v[e], y[e], scale);
       }
       __nv_bfloat16 t[4][3];
 #pragma unroll
@@ -60,8 +75,10 @@ __global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda,
 // rows of B (float2 per lane); each lane stores two consecutive k of one
 // output row as a 4-byte pair, so a warp writes 128 contiguous bytes per
 // plane.
+template <int MODE>
 __global__ void split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
-                                       int nterms, __nv_bfloat16* __restrict__ out) {
+                                       int nterms, __nv_bfloat16* __restrict__ out, const float* __restrict__ Y,
+                                       int64_t ldy, float scale) {
   __shared__ float tile[64][65];
   const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
   const int64_t plane = (int64_t)ncols * kpad;
@@ -76,6 +93,16 @@ __global__ void split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb,
         v = *reinterpret_cast<const float2*>(src);  // n even, ldb % 4 == 0: 8-byte aligned
       } else if (n < ncols) {
         v.x = src[0];
+      }
+      if constexpr (MODE != kXformNone) {
+        const float* ysrc = Y + (int64_t)k * ldy + n;
+        float2 y = make_float2(0.f, 0.f);
+        if (n + 1 < ncols)
+          y = *reinterpret_cast<const float2*>(ysrc);
+        else if (n < ncols)
+          y.x = ysrc[0];
+        v.x = xform<MODE>(v.x, y.x, scale);
+        v.y = xform<MODE>(v.y, y.y, scale);
       }
     }
     tile[i][2 * tx] = v.x;
@@ -187,18 +214,31 @@ static unsigned grid_for(int64_t work, int threads, int sms) {
   return (unsigned)std::max<int64_t>(b, 1);
 }
 
-cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
-                              bool transpose, int sms, cudaStream_t st) {
+template <int MODE>
+static void split_bf16_launch(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
+                              bool transpose, int sms, cudaStream_t st, const float* Y, int64_t ldy, float scale) {
   if (!transpose) {
     const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(ceil_div(kpad / 4, 256), 16));
     const int64_t gy = std::max<int64_t>(1, std::min<int64_t>({(int64_t)rows, (int64_t)sms * 16 / gx, 65535}));
-    split_bf16_rows_kernel<<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(A, lda, rows, cols, kpad, nterms,
-                                                                               static_cast<__nv_bfloat16*>(out));
+    split_bf16_rows_kernel<MODE><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(
+        A, lda, rows, cols, kpad, nterms, static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
   } else {
     // A is K x N here (krows = rows, ncols = cols); output N x kpad.
     dim3 grid((unsigned)ceil_div(cols, 64), (unsigned)ceil_div(kpad, 64));
-    split_bf16_cols_kernel<<<grid, dim3(32, 8), 0, st>>>(A, lda, rows, cols, kpad, nterms,
-                                                         static_cast<__nv_bfloat16*>(out));
+    split_bf16_cols_kernel<MODE><<<grid, dim3(32, 8), 0, st>>>(A, lda, rows, cols, kpad, nterms,
+                                                               static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
+  }
+}
+
+cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
+                              bool transpose, int sms, cudaStream_t st, int xform, const float* Y, int64_t ldy,
+                              float scale) {
+  switch (xform) {
+    case kXformNone: split_bf16_launch<kXformNone>(A, lda, rows, cols, kpad, nterms, out, transpose, sms, st, Y, ldy, scale); break;
+    case kXformScale: split_bf16_launch<kXformScale>(A, lda, rows, cols, kpad, nterms, out, transpose, sms, st, Y, ldy, scale); break;
+    case kXformSigmoidGrad: split_bf16_launch<kXformSigmoidGrad>(A, lda, rows, cols, kpad, nterms, out, transpose, sms, st, Y, ldy, scale); break;
+    case kXformReluGrad: split_bf16_launch<kXformReluGrad>(A, lda, rows, cols, kpad, nterms, out, transpose, sms, st, Y, ldy, scale); break;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }

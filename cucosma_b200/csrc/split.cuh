@@ -11,8 +11,16 @@ namespace cucosma {
 // FP32 rows x cols -> nterms BF16 planes.  transpose = false: planes are
 // [nterms][rows][kpad] (A operand, cols = K).  transpose = true: the input is
 // K x N (rows = K, cols = N) and planes are [nterms][N][kpad] (B operand).
+//
+// xform (backward pass): the value split is not A[i] but
+//   kXformScale:        scale * A[i]
+//   kXformSigmoidGrad:  scale * A[i] * Y[i] * (1 - Y[i])   (A = dY, Y = sigmoid output)
+//   kXformReluGrad:     Y[i] > 0 ? scale * A[i] : 0        (Y = ReLU output)
+// with Y read at the same (row, column) as A (row stride ldy).
+enum SplitXform : int { kXformNone = 0, kXformScale = 1, kXformSigmoidGrad = 2, kXformReluGrad = 3 };
 cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
-                              bool transpose, int sms, cudaStream_t st);
+                              bool transpose, int sms, cudaStream_t st, int xform = kXformNone,
+                              const float* Y = nullptr, int64_t ldy = 0, float scale = 1.0f);
 
 // Per-row exponents of A (m x k) and per-column exponents of B (k x n).
 cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,

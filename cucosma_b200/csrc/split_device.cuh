@@ -56,4 +56,13 @@ __device__ __forceinline__ int64_t packed_index(int64_t r, int k, int64_t kpad, 
   return r * (kpad * S) + (int64_t)(k >> 5) * (32 * S) + p * 32 + (k & 31);
 }
 
+// Backward-pass source transforms of the BF16 split (see SplitXform).
+template <int MODE>
+__device__ __forceinline__ float xform(float v, float y, float scale) {
+  if constexpr (MODE == 1) return scale * v;
+  if constexpr (MODE == 2) return scale * v * (y * (1.0f - y));
+  if constexpr (MODE == 3) return y > 0.0f ? scale * v : 0.0f;
+  return v;
+}
+
 }  // namespace cucosma

@@ -127,7 +127,13 @@ void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan
 
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                        const DeviceInfo* di, cudaStream_t st) {
+  return tc_gemm_ex(d, A, B, C, ws, di, st, false);
+}
+
+cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
+                          const DeviceInfo* di, cudaStream_t st, bool planes_ready) {
   const Plan pl = make_plan(d, di);
+  if (planes_ready && pl.kind == 2) return CUCOSMA_STATUS_NOT_SUPPORTED;
   if (pl.kind == 2 && (pl.slices < 4 || pl.slices > 9)) return CUCOSMA_STATUS_NOT_SUPPORTED;
   uint8_t* w = static_cast<uint8_t*>(ws);
   const int m = (int)d->m, n = (int)d->n, k = (int)d->k;
@@ -162,11 +168,13 @@ cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B,
   int launches = 0;
   if (pl.kind != 2) {
     const int nt = pl.slices;
-    e = launch_split_bf16((const float*)A, d->lda, m, k, pl.kpad, nt, w + pl.off_a, false, di->sms, st);
-    if (e == cudaSuccess)
-      e = launch_split_bf16((const float*)B, d->ldb, k, n, pl.kpad, nt, w + pl.off_b, true, di->sms, st);
-    launches += 2;
-    if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    if (!planes_ready) {
+      e = launch_split_bf16((const float*)A, d->lda, m, k, pl.kpad, nt, w + pl.off_a, false, di->sms, st);
+      if (e == cudaSuccess)
+        e = launch_split_bf16((const float*)B, d->ldb, k, n, pl.kpad, nt, w + pl.off_b, true, di->sms, st);
+      launches += 2;
+      if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    }
     if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, w + pl.off_a, k, m, nt, pl.kpad, (uint64_t)m * pl.kpad,
                    pl.bk, 128, nt, CU_TENSOR_MAP_SWIZZLE_64B) ||
         !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, w + pl.off_b, k, n, nt, pl.kpad, (uint64_t)n * pl.kpad,

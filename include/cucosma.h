@@ -121,6 +121,22 @@ CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
                              double beta, double* C, int ldc, void* stream);
 
+/* --------------------------------------------------------------- backward
+ * Gradients of the forward Y = epi(alpha*A*B + beta*C0) computed by
+ * cucosma_gemm with descriptor *fwd (FP32, precision BF16X3 or BF16X6; no
+ * counterpart in the reference, which has no backward pass).  Saved operands
+ * A, B and the forward output Y (row stride ldy; unused when the epilogue is
+ * NONE) and the upstream gradient dY give
+ *     G  = alpha * dY (.) epi'(Z),  epi' = Y(1-Y) (sigmoid), [Y > 0] (ReLU), 1
+ *     dA = G * B^T   (m x k, row stride ldda)      dB = A^T * G   (k x n, lddb)
+ * on the tensor cores, with epi' fused into the operand pre-pass; either of
+ * dA / dB may be NULL to skip it.  Overwrites dA and dB. */
+CUCOSMA_API cucosma_status cucosma_gemm_backward_workspace_size(const cucosma_gemm_desc* fwd, size_t* bytes);
+CUCOSMA_API cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* fwd, const void* A, const void* B,
+                                                 const void* Y, int64_t ldy, const void* dY, int64_t lddy, void* dA,
+                                                 int64_t ldda, void* dB, int64_t lddb, void* workspace,
+                                                 size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- grouped
  * Many independent GEMMs of uneven sizes in one persistent launch (no
  * counterpart in the reference, whose sizes are compile-time macros: one
