@@ -224,6 +224,45 @@ def profile_stop():
     return ms.value, n.value
 
 
+def tune(A, B, Cm, alpha=1.0, beta=0.0, precision="native", slices=0, max_candidates=0, workspace=None,
+         stream=None):
+    """Measure candidate configurations of this GEMM on the device and cache
+    the fastest (C is overwritten).  Returns the cucosma_tune_result fields."""
+    import torch
+
+    from ._ext import TuneResult
+
+    d = make_desc(A, B, Cm, alpha, beta, precision=precision, slices=slices)
+    if workspace is None:
+        # room for the largest split-K candidate
+        biggest = 0
+        for sk in (1, 2, 4, 8, 16, 32, 64):
+            dd = make_desc(A, B, Cm, alpha, beta, precision=precision, slices=slices, split_k=sk)
+            biggest = max(biggest, workspace_size(dd))
+        workspace = torch.empty(max(biggest, 256), dtype=torch.uint8, device=Cm.device)
+    r = TuneResult()
+    check(lib().cucosma_tune(C.byref(d), A.data_ptr(), B.data_ptr(), Cm.data_ptr(), workspace.data_ptr(),
+                             workspace.numel(), int(max_candidates), C.byref(r), _stream_handle(stream)),
+          "cucosma_tune")
+    return r.as_dict()
+
+
+def tune_cache_save(path):
+    check(lib().cucosma_tune_cache_save(os.fsencode(path)), "cucosma_tune_cache_save")
+
+
+def tune_cache_load(path):
+    check(lib().cucosma_tune_cache_load(os.fsencode(path)), "cucosma_tune_cache_load")
+
+
+def tune_cache_clear():
+    check(lib().cucosma_tune_cache_clear(), "cucosma_tune_cache_clear")
+
+
+def tune_cache_size():
+    return int(lib().cucosma_tune_cache_size())
+
+
 def gemm_backward(A, B, Y, dY, dA=None, dB=None, alpha=1.0, precision="bf16x3", epilogue="sigmoid", workspace=None,
                   stream=None):
     """Gradients of Y = epi(alpha*A@B + beta*C0): dA = G@B^T, dB = A^T@G with

@@ -5,6 +5,17 @@ from __future__ import annotations
 import ctypes as C
 
 
+class TuneResult(C.Structure):
+    """Mirror of cucosma_tune_result."""
+
+    _fields_ = [("split_k", C.c_int32), ("swizzle", C.c_int32), ("tile", C.c_int32), ("candidates", C.c_int32),
+                ("occupancy", C.c_int32), ("reserved", C.c_int32), ("ms", C.c_double), ("tflops", C.c_double),
+                ("l2_reuse_model", C.c_double)]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "reserved"}
+
+
 class Problem(C.Structure):
     """Mirror of cucosma_gemm_problem."""
 
@@ -22,6 +33,11 @@ def bind(L):
         "cucosma_grouped_plan_create": ([C.POINTER(GemmDesc), P, C.c_int, vp, sz, C.POINTER(vp)], C.c_int),
         "cucosma_gemm_grouped": ([vp, vp], C.c_int),
         "cucosma_grouped_plan_destroy": ([vp], C.c_int),
+        "cucosma_tune": ([C.POINTER(GemmDesc), vp, vp, vp, vp, sz, C.c_int, C.POINTER(TuneResult), vp], C.c_int),
+        "cucosma_tune_cache_save": ([C.c_char_p], C.c_int),
+        "cucosma_tune_cache_load": ([C.c_char_p], C.c_int),
+        "cucosma_tune_cache_clear": ([], C.c_int),
+        "cucosma_tune_cache_size": ([], C.c_int),
         "cucosma_gemm_backward_workspace_size": ([C.POINTER(GemmDesc), C.POINTER(sz)], C.c_int),
         "cucosma_gemm_backward": ([C.POINTER(GemmDesc), vp, vp, vp, C.c_int64, vp, C.c_int64, vp, C.c_int64, vp,
                                    C.c_int64, vp, sz, vp], C.c_int),

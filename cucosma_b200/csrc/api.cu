@@ -231,6 +231,8 @@ cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, vo
   const DeviceInfo* di = device_info();
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (di->cc_major != 10 || di->cc_minor != 0) return CUCOSMA_STATUS_ARCH_MISMATCH;
+  cucosma_gemm_desc tuned;
+  d = apply_tuning(d, &tuned, di);
   const bool fp32 = d->dtype == CUCOSMA_R_32F;
   if (d->k == 0 || d->alpha == 0.0) {
     cudaError_t e = fp32 ? simt::launch_scale<float>((float*)C, d->ldc, (int)d->m, (int)d->n, d->beta, d->epilogue,
@@ -328,7 +330,8 @@ extern "C" cucosma_status cucosma_gemm_workspace_size(const cucosma_gemm_desc* d
   if (!d || d->m < 0 || d->n < 0 || d->k < 0) return CUCOSMA_STATUS_INVALID_VALUE;
   const DeviceInfo* di = device_info();
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
-  return workspace_size(d, bytes, di);
+  cucosma_gemm_desc tuned;
+  return workspace_size(apply_tuning(d, &tuned, di), bytes, di);
 }
 
 extern "C" cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cucosma_plan_info* info) {
@@ -337,6 +340,8 @@ extern "C" cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cuco
   std::memset(info, 0, sizeof(*info));
   const DeviceInfo* di = device_info();
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  cucosma_gemm_desc tuned;
+  d = apply_tuning(d, &tuned, di);
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
     const NativePlan pl = plan_native(d, di->sms);
     info->path = 0;

@@ -49,6 +49,10 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
 
 void* managed_workspace(size_t bytes);
 
+// Tuning cache (tune.cu): when d leaves split_k, swizzle and tile at 0 and the
+// cache holds a choice for it, returns tmp filled with that choice, else d.
+const cucosma_gemm_desc* apply_tuning(const cucosma_gemm_desc* d, cucosma_gemm_desc* tmp, const DeviceInfo* di);
+
 // Launch accounting and optional timing of the main GEMM kernel of each call:
 // note_launches() counts every kernel the library enqueues; prof_begin /
 // prof_end bracket the main kernel with CUDA events while profiling is on.

@@ -303,6 +303,18 @@ cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, 
   return cudaGetLastError();
 }
 
+template <typename T>
+int occupancy() {
+  const size_t smem = smem_bytes<T>();
+  cudaFuncSetAttribute(simt_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, simt_gemm_kernel<T>, kThreads, smem) != cudaSuccess)
+    return 0;
+  return blocks;
+}
+template int occupancy<float>();
+template int occupancy<double>();
+
 template cudaError_t launch_gemm<float>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
 template cudaError_t launch_gemm<double>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
 template cudaError_t launch_reduce<float>(const float*, int64_t, int64_t, int, float*, int64_t, int, int, double, double,

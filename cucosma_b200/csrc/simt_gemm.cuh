@@ -45,6 +45,9 @@ struct Cfg<double> {
 
 template <typename T>
 size_t smem_bytes();
+// Resident CTAs per SM of the GEMM kernel (CUDA occupancy API).
+template <typename T>
+int occupancy();
 template <typename T>
 cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, cudaStream_t stream);
 template <typename T>

@@ -121,6 +121,33 @@ CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,
                              double beta, double* C, int ldc, void* stream);
 
+/* ------------------------------------------------------------------ tuner
+ * Replaces the reference's ScheduleGenerator (ScheduleGenerator/
+ * ScheduleGeneratorv4.h:13, a host-side brute force ranked by a
+ * communication-volume model): candidate split-K factors, raster bands /
+ * block-index remap widths and tile variants of *d are run on the device on
+ * the caller's buffers (C is overwritten: pass scratch) and the fastest is
+ * cached for (SM count, dtype, precision, slices, m, n, k).  Candidates whose
+ * workspace exceeds workspace_bytes are skipped; max_candidates <= 0 = all.
+ * cucosma_gemm uses the cached choice whenever split_k, swizzle and tile are
+ * all 0.  The cache is saved / loaded as a text file; $CUCOSMA_TUNE_CACHE is
+ * loaded on first use, CUCOSMA_TUNE=off disables lookups. */
+typedef struct cucosma_tune_result {
+  int32_t split_k, swizzle, tile; /* the chosen configuration */
+  int32_t candidates;             /* configurations measured */
+  int32_t occupancy;              /* resident CTAs per SM of the chosen kernel */
+  int32_t reserved;
+  double ms, tflops;              /* measured time of one call of the chosen configuration */
+  double l2_reuse_model;          /* modelled fraction of operand-tile loads served by L2 */
+} cucosma_tune_result;
+CUCOSMA_API cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
+                                        void* workspace, size_t workspace_bytes, int max_candidates,
+                                        cucosma_tune_result* out, void* stream);
+CUCOSMA_API cucosma_status cucosma_tune_cache_save(const char* path);
+CUCOSMA_API cucosma_status cucosma_tune_cache_load(const char* path);
+CUCOSMA_API cucosma_status cucosma_tune_cache_clear(void);
+CUCOSMA_API int cucosma_tune_cache_size(void);
+
 /* --------------------------------------------------------------- backward
  * Gradients of the forward Y = epi(alpha*A*B + beta*C0) computed by
  * cucosma_gemm with descriptor *fwd (FP32, precision BF16X3 or BF16X6; no

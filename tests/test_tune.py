@@ -1,0 +1,69 @@
+"""The autotuner (cucosma_tune) and its cache.  CPU: the cache file format
+round-trips without a GPU.  GPU: tuning measures several candidates, records
+the fastest, and later auto-configured calls use it and stay correct."""
+import os
+
+import numpy as np
+import pytest
+
+import cucosma_b200 as cc
+import oracle
+from tests._util import check_against_oracle, to_dev, uniform
+
+LINES = ["v1 148 0 0 0 1024 1024 1024 3 1 0 0.123000", "v1 148 0 1 0 8192 8192 8192 1 8 0 2.500000"]
+
+
+def test_cache_file_roundtrip(tmp_path):
+    cc.tune_cache_clear()
+    src = tmp_path / "in.txt"
+    src.write_text("\n".join(LINES) + "\n")
+    cc.tune_cache_load(str(src))
+    assert cc.tune_cache_size() == 2
+    out = tmp_path / "out.txt"
+    cc.tune_cache_save(str(out))
+    assert sorted(out.read_text().strip().splitlines()) == sorted(LINES)
+    cc.tune_cache_clear()
+    assert cc.tune_cache_size() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,dtype", [("native", np.float32), ("bf16x3", np.float32), ("native", np.float64)])
+def test_tune_then_use(cuda, tmp_path, precision, dtype):
+    import torch
+
+    cc.tune_cache_clear()
+    m, n, k = 384, 320, 6000
+    A, B = uniform(1, (m, k), dtype), uniform(2, (k, n), dtype)
+    Cin = uniform(3, (m, n), dtype)
+    dA, dB = to_dev(A), to_dev(B)
+    scratch = to_dev(np.zeros((m, n), dtype))
+    r = cc.tune(dA, dB, scratch, 1.0, 0.5, precision=precision)
+    print(precision, r)
+    assert r["candidates"] >= 3 and r["ms"] > 0 and r["tflops"] > 0 and r["occupancy"] >= 1
+    assert 0.0 <= r["l2_reuse_model"] <= 1.0
+    assert cc.tune_cache_size() == 1
+    dC = to_dev(Cin)
+    plan = cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))
+    assert plan["splits"] == r["split_k"] or r["split_k"] > plan["splits"] == (-(-k // plan["tile_k"]))
+    cc.gemm(dA, dB, dC, 1.0, 0.5, precision=precision)
+    torch.cuda.synchronize()
+    out = dC.cpu().numpy()
+    if precision == "native":
+        check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_NONE, dtype)
+    else:
+        ref = oracle.gemm(A, B, Cin, 1.0, 0.5)
+        assert oracle.errors(out, ref)["normwise"] < 1e-4
+    path = tmp_path / "cache.txt"
+    cc.tune_cache_save(str(path))
+    cc.tune_cache_clear()
+    cc.tune_cache_load(str(path))
+    assert cc.tune_cache_size() == 1
+    os.environ["CUCOSMA_TUNE"] = "off"
+    try:
+        p_off = cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))
+    finally:
+        del os.environ["CUCOSMA_TUNE"]
+    p_on = cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))
+    assert p_on["splits"] == plan["splits"]
+    cc.tune_cache_clear()
+    assert p_off["splits"] == cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))["splits"]
