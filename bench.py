@@ -206,6 +206,37 @@ def e2e_path(cc, A_h, B_h, C_h, A, B, Cm, prec, slices, steps, warmup, workspace
     return e0.elapsed_time(e1) / steps
 
 
+def fwd_bwd_bench(cc, steps, warmup, n=4096, precision="bf16x3"):
+    """Forward Y = sigmoid(A@B) and backward dA, dB (three GEMMs of n^3),
+    A, B uniform[-0.1, 0.1], dY uniform[-1, 1]; one step = forward + backward."""
+    import torch
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    A = (torch.rand((n, n), generator=g, device="cuda") * 2 - 1) * 0.1
+    B = (torch.rand((n, n), generator=g, device="cuda") * 2 - 1) * 0.1
+    dY = torch.rand((n, n), generator=g, device="cuda") * 2 - 1
+    Y, dA, dB = (torch.empty((n, n), device="cuda") for _ in range(3))
+    ws_f = cc.alloc_workspace(cc.make_desc(A, B, Y, precision=precision, epilogue="sigmoid"))
+
+    def step():
+        cc.gemm(A, B, Y, 1.0, 0.0, precision=precision, epilogue="sigmoid", workspace=ws_f)
+        cc.gemm_backward(A, B, Y, dY, dA, dB, precision=precision, epilogue="sigmoid")
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"n": n, "precision": precision, "ms": ms, "tflops": 3 * 2.0 * n ** 3 / ms / 1e9,
+            "what": "Y = sigmoid(A@B), dA = G@B^T, dB = A^T@G, G = dY*Y*(1-Y) fused"}
+
+
 def grouped_shapes(count=512, seed=5):
     """512 GEMMs: M, N log-uniform in [64, 2048], K log-uniform in [64, 8192]."""
     r = np.random.default_rng(seed)
@@ -370,8 +401,47 @@ def reference_arm(args):
             "config": {"workload": "reference CPU product, sample of the %d^3 GEMM" % n, "m": n, "n": n, "k": n},
             "cpu_baseline": {"value": tflops, "unit": "TFLOP/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": tflops, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gk = reference_gpu_kernel(n, args.steps, args.warmup)
+    if gk:
+        line["reference_gpu_kernel"] = gk
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu_kernel(n, steps, warmup):
+    """Informational: the reference kernel cosmaSgemm compiled unmodified for
+    sm_100a from its sources (oracle/_ref, 8192^3, alpha 1, beta 0.5, tiles
+    from its ScheduleGenerator) timed with CUDA events -- the plain FP32 kernel
+    the precision paths are compared with.  Absent when not built or no GPU."""
+    try:
+        import torch
+
+        import oracle
+
+        tag = "f32_%d_a1b05" % n
+        if not torch.cuda.is_available() or tag not in oracle.ref_kernel_tags():
+            return None
+        ref = oracle.RefKernel(tag)
+        ld = -(-n // 128) * 128  # cudaMallocPitch-like rows
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1)
+        A = (torch.rand((n, ld), generator=g, device="cuda") * 2 - 1)
+        B = (torch.rand((n, ld), generator=g, device="cuda") * 2 - 1)
+        C = torch.zeros((n, ld), device="cuda")
+        for _ in range(max(1, warmup)):
+            ref(A.data_ptr(), ld, B.data_ptr(), ld, C.data_ptr(), ld)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            ref(A.data_ptr(), ld, B.data_ptr(), ld, C.data_ptr(), ld)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        return {"what": "cosmaSgemm (cuCOSMAV100.cuh) built for sm_100a, %d^3 FP32 SIMT, config %s" % (n, ref.config),
+                "ms": ms, "tflops": 2.0 * n ** 3 / ms / 1e9}
+    except Exception as e:  # informational only
+        return {"error": str(e)[:200]}
 
 
 # -------------------------------------------------------------------- main
@@ -385,7 +455,7 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / error leg")
     ap.add_argument("--only", default="", help="comma-separated subset of paths (profiling runs): "
-                    "bf16x3,bf16x6,native_f32,ozaki,native_f64,grouped_bf16x3,grouped_ozaki")
+                    "bf16x3,bf16x6,native_f32,ozaki,native_f64,grouped_bf16x3,grouped_ozaki,fwd_bwd")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -453,6 +523,8 @@ def main():
                                    ("grouped_ozaki", "ozaki", torch.float64, OZAKI_SLICES)):
         if not args.only or gname in args.only.split(","):
             results[gname] = grouped_bench(cc, gprec, gdt, gsl, max(3, args.steps), args.warmup, seed=5 + 10 * rank)
+    if not args.only or "fwd_bwd" in args.only.split(","):
+        results["fwd_bwd_bf16x3"] = fwd_bwd_bench(cc, max(3, args.steps), args.warmup)
     avail = [p for p in paths if results.get(p[0], {}).get("available")]
     if not avail:  # a profiling run of the grouped launches only
         clocks = sampler.stop()
