@@ -2,35 +2,46 @@
 //
 // Replaces the reference kernel cosmaSgemm_kernel (cuCOSMAV100.cuh:2505-2756)
 // and its split-K reduction (cosmaSplitKReduce.cuh:20-58) with a B200 design:
-//   * a producer warp streams A and B tiles with TMA into a 4-stage shared
-//     memory ring guarded by mbarriers (the reference double-buffers with
+//   * thread 0 streams A and B tiles with TMA into a 4-stage shared memory
+//     ring guarded by mbarriers (the reference double-buffers with
 //     __syncthreads and register-staged loads that transpose A on the way);
-//   * A tiles land row-major with the 64-byte TMA swizzle, so the compute
-//     warps read 8 rows x VEC k-values per LDS.128 without bank conflicts and
-//     no transposition is needed;
-//   * 8 compute warps hold a 128x128 CTA tile, 8x8 outputs per thread, rows
-//     interleaved by 4 within a warp's 32 rows;
+//   * A tiles land row-major with the 64-byte TMA swizzle (conflict-free
+//     16-byte reads of any row);
+//   * FP64 (simt_gemm_kernel<double>) reads 2 k-values of 8 rows per step
+//     straight from the swizzled tile; FP32 (simt_sgemm_kernel) first
+//     transposes each A stage into a k-major buffer, so a k-step is 4 LDS.128
+//     feeding 64 FFMA, and runs two CTAs per SM at 128 registers;
+//   * 8 compute warps hold a 128x128 CTA tile, 8x8 outputs per thread;
 //   * split-K writes raw partial tiles to a caller-provided workspace and a
 //     separate kernel reduces them in ascending split order (deterministic),
 //     then applies alpha/beta and the epilogue, like cosmaSplitKReduce;
 //   * the block-index swizzle follows the reference's remap
 //     (cuCOSMAV100.cuh:2586-2603).
+#include <type_traits>
+
 #include "simt_gemm.cuh"
 
 namespace cucosma {
 
 template <typename T>
-__global__ void __launch_bounds__(simt::kThreads, 1)
+__device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParams& p, const int (&rows)[8], int c0);
+
+template <typename T>
+__global__ void __launch_bounds__(simt::kThreads, simt::Cfg<T>::MIN_BLOCKS)
     simt_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      const SimtParams p) {
   using namespace simt;
   constexpr int BK = Cfg<T>::BK;
   constexpr int VEC = Vec<T>::n;
   using V = typename Vec<T>::type;
+  // A fragments cover KV = 2 consecutive k per row (an 8-byte load for FP32,
+  // 16-byte for FP64): 2 * (8 + 8) fragment registers, so FP32 fits 128
+  // registers and two CTAs per SM.
+  constexpr int KV = 2;
+  using AV = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
   constexpr int A_STAGE = BM * BK * (int)sizeof(T);
   constexpr int B_STAGE = BK * BN * (int)sizeof(T);
-  constexpr int KG = BK / VEC;  // k-groups per stage (one LDS.128 of A covers VEC k)
-  static_assert(KG == 4, "stage holds four 16-byte chunks per A row");
+  constexpr int KG = BK / KV;  // k-groups per stage
   static_assert(BK * sizeof(T) == 64, "A rows are 64 bytes (64-byte swizzle span)");
 
   extern __shared__ uint8_t smem_raw[];
@@ -95,15 +106,11 @@ __global__ void __launch_bounds__(simt::kThreads, 1)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
 
-  // Byte offsets (within a stage) of this thread's A rows (swizzle applied
-  // per chunk) and B columns.
-  int a_row_off[8], a_sw[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = wm * 32 + ty + 4 * i;
-    a_row_off[i] = r * 64;
-    a_sw[i] = (r >> 1) & 3;
-  }
+  // This thread's A rows are r_i = wm*32 + ty + 4i (64-byte rows, byte
+  // offset a_base + 256 i); the 64-byte swizzle XORs the 16-byte chunk index
+  // with (r_i >> 1) & 3, which is sw0 for even i and sw0 ^ 2 for odd i.
+  const int a_base = (wm * 32 + ty) * 64;
+  const int sw0 = (ty >> 1) & 3;
   constexpr int NJ = 8 / VEC;  // vectors per thread along N
   const int b_col = wn * 64 + tx * VEC;
 
@@ -118,27 +125,31 @@ __global__ void __launch_bounds__(simt::kThreads, 1)
     const T* bs = reinterpret_cast<const T*>(Bs + s * B_STAGE);
 #pragma unroll
     for (int kg = 0; kg < KG; ++kg) {
-      T a[8][VEC];
-      T b[VEC][8];
+      // KV consecutive k of 8 A rows (one 8- or 16-byte load each) and the
+      // 8 B columns of those k: KV * 64 FMAs.
+      const int kb_off = kg * KV * (int)sizeof(T);  // byte offset of k-group kg inside a 64-byte row
+      T a[8][KV];
+      T b[KV][8];
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const V v = *reinterpret_cast<const V*>(as + a_row_off[i] + ((kg ^ a_sw[i]) << 4));
+        const int sw = (i & 1) ? (sw0 ^ 2) : sw0;
+        const AV v = *reinterpret_cast<const AV*>(as + a_base + 256 * i + ((((kb_off >> 4) ^ sw) << 4) | (kb_off & 15)));
         const T* pv = reinterpret_cast<const T*>(&v);
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) a[i][e] = pv[e];
+        for (int e = 0; e < KV; ++e) a[i][e] = pv[e];
       }
 #pragma unroll
-      for (int kk = 0; kk < VEC; ++kk) {
+      for (int kk = 0; kk < KV; ++kk) {
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
-          const V v = *reinterpret_cast<const V*>(bs + (kg * VEC + kk) * BN + b_col + j * 8 * VEC);
+          const V v = *reinterpret_cast<const V*>(bs + (kg * KV + kk) * BN + b_col + j * 8 * VEC);
           const T* pv = reinterpret_cast<const T*>(&v);
 #pragma unroll
           for (int e = 0; e < VEC; ++e) b[kk][j * VEC + e] = pv[e];
         }
       }
 #pragma unroll
-      for (int kk = 0; kk < VEC; ++kk)
+      for (int kk = 0; kk < KV; ++kk)
 #pragma unroll
         for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -156,15 +167,28 @@ __global__ void __launch_bounds__(simt::kThreads, 1)
     return;
   }
 
-  // --------------------------------------------------------------- epilogue
+  int rows[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) rows[i] = m0 + wm * 32 + ty + 4 * i;
+  simt_store<T>(acc, p, rows, n0 + b_col);
+}
+
+// Epilogue of the SIMT kernels: this thread's 8 x 8 accumulators, rows
+// rows[i], columns c0 + j*8*VEC + [0, VEC) for j < 8/VEC; either raw partial
+// sums into the split-K workspace or epi(alpha*acc + beta*C) into C.
+template <typename T>
+__device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParams& p, const int (&rows)[8], int c0) {
+  constexpr int VEC = Vec<T>::n;
+  constexpr int NJ = 8 / VEC;
+  using V = typename Vec<T>::type;
   const T alpha = (T)p.alpha, beta = (T)p.beta;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const int r = m0 + wm * 32 + ty + 4 * i;
+    const int r = rows[i];
     if (r >= p.m) continue;
 #pragma unroll
     for (int j = 0; j < NJ; ++j) {
-      const int c = n0 + b_col + j * 8 * VEC;
+      const int c = c0 + j * 8 * VEC;
       if (c >= p.n) continue;
       if (p.partial) {
         T* w = reinterpret_cast<T*>(p.out) + (int64_t)blockIdx.z * p.ws_split_stride + (int64_t)r * p.ldo + c;
@@ -198,6 +222,136 @@ __global__ void __launch_bounds__(simt::kThreads, 1)
       }
     }
   }
+}
+
+// FP32 kernel.  Same TMA/mbarrier ring as simt_gemm_kernel, but every A
+// stage is transposed once in shared memory into a k-major buffer (double
+// buffered, one CTA barrier per stage), so each k costs 2 LDS.128 for the 8 A
+// values and 2 for the 8 B values of a thread's 8x8 tile (thread rows are two
+// groups of 4 consecutive rows).  128 registers: two CTAs per SM.
+namespace simt {
+constexpr int kLdT = BM + 4;  // k-major A row pitch (floats): 16-byte aligned rows
+}
+
+__global__ void __launch_bounds__(simt::kThreads, 2)
+    simt_sgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const SimtParams p) {
+  using namespace simt;
+  constexpr int BK = Cfg<float>::BK;  // 16
+  constexpr int A_STAGE = BM * BK * 4, B_STAGE = BK * BN * 4;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* As = smem;
+  uint8_t* Bs = smem + STAGES * A_STAGE;
+  float* AsT = reinterpret_cast<float*>(smem + STAGES * (A_STAGE + B_STAGE));  // [2][BK][kLdT]
+  uint64_t* full = reinterpret_cast<uint64_t*>(AsT + 2 * BK * kLdT);
+  uint64_t* empty = full + STAGES;
+
+  int tile_n, tile_m;  // block-index remap, cuCOSMAV100.cuh:2586-2603
+  if (p.swizzle > 1) {
+    tile_n = blockIdx.x / p.swizzle;
+    tile_m = blockIdx.y * p.swizzle + blockIdx.x % p.swizzle;
+    if (tile_m >= p.tiles_m) return;
+  } else {
+    tile_n = blockIdx.x;
+    tile_m = blockIdx.y;
+  }
+  const int m0 = tile_m * BM, n0 = tile_n * BN;
+  const int64_t kbeg = (int64_t)blockIdx.z * p.kchunk;
+  const int64_t kend = min((int64_t)p.k, kbeg + p.kchunk);
+  const int nkb = kend > kbeg ? (int)ceil_div(kend - kbeg, BK) : 0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kComputeWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  int issued = 0;
+  auto produce = [&](int kb) -> bool {
+    const int s = kb % STAGES;
+    if (!mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1, kErrTimeoutEmpty, p.ctl)) return false;
+    mbar_arrive_expect_tx(&full[s], A_STAGE + B_STAGE);
+    const int kx = (int)(kbeg + (int64_t)kb * BK);
+    tma_load_2d(As + s * A_STAGE, &tmA, kx, m0, &full[s]);
+    tma_load_2d(Bs + s * B_STAGE, &tmB, n0, kx, &full[s]);
+    issued = kb + 1;
+    return true;
+  };
+  bool ok = true;
+  if (tid == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+    for (int kb = 0; kb < min(nkb, STAGES - 1) && ok; ++kb) ok = produce(kb);
+  }
+
+  const int wm = warp >> 1, wn = warp & 1;
+  const int tx = lane & 7, ty = lane >> 3;
+  const int a_col = wm * 32 + ty * 4;  // this thread's rows: a_col + {0..3}, a_col + 16 + {0..3}
+  const int b_col = wn * 64 + tx * 4;  // columns: b_col + {0..3}, b_col + 32 + {0..3}
+  // transpose role: thread handles row tr, k-half th (8 consecutive k)
+  const int tr = tid & (BM - 1), th = tid >> 7;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+  for (int kb = 0; kb < nkb; ++kb) {
+    bool good = ok;
+    if (tid == 0 && good && kb + STAGES - 1 < nkb) good = produce(kb + STAGES - 1);
+    const int s = kb % STAGES;
+    if (good) good = mbar_wait(&full[s], (kb / STAGES) & 1, kErrTimeoutFull, p.ctl);
+    float* at = AsT + (kb & 1) * BK * kLdT;
+    if (good) {
+      // two 16-byte chunks of row tr (64-byte swizzle: chunk ^ ((tr >> 1) & 3))
+      const uint8_t* arow = As + s * A_STAGE + tr * 64;
+      const int sw = (tr >> 1) & 3;
+      const float4 q0 = *reinterpret_cast<const float4*>(arow + (((2 * th) ^ sw) << 4));
+      const float4 q1 = *reinterpret_cast<const float4*>(arow + (((2 * th + 1) ^ sw) << 4));
+      float* col = at + th * 8 * kLdT + tr;
+      col[0 * kLdT] = q0.x;
+      col[1 * kLdT] = q0.y;
+      col[2 * kLdT] = q0.z;
+      col[3 * kLdT] = q0.w;
+      col[4 * kLdT] = q1.x;
+      col[5 * kLdT] = q1.y;
+      col[6 * kLdT] = q1.z;
+      col[7 * kLdT] = q1.w;
+    }
+    // Uniform across the CTA: nobody leaves the loop while others wait here.
+    ok = __syncthreads_and(good);
+    if (!ok) break;
+    const float* bs = reinterpret_cast<const float*>(Bs + s * B_STAGE);
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      const float4 a0 = *reinterpret_cast<const float4*>(at + k * kLdT + a_col);
+      const float4 a1 = *reinterpret_cast<const float4*>(at + k * kLdT + a_col + 16);
+      const float4 b0 = *reinterpret_cast<const float4*>(bs + k * BN + b_col);
+      const float4 b1 = *reinterpret_cast<const float4*>(bs + k * BN + b_col + 32);
+      const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok) {
+    if (tid == 0)
+      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
+        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, kErrTimeoutDrain, p.ctl);
+    return;
+  }
+  int rows[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) rows[i] = m0 + a_col + (i & 3) + (i >> 2) * 16;
+  simt_store<float>(acc, p, rows, n0 + b_col);
 }
 
 // Deterministic split-K reduction: C = epi(alpha * sum_z ws[z] + beta*C),
@@ -259,7 +413,17 @@ namespace simt {
 template <typename T>
 size_t smem_bytes() {
   constexpr int BK = Cfg<T>::BK;
-  return 1024 + STAGES * (BM * BK + BK * BN) * sizeof(T) + 2 * STAGES * sizeof(uint64_t);
+  // FP32 adds the double-buffered k-major copy of A
+  constexpr size_t transposed = std::is_same<T, float>::value ? 2 * BK * kLdT * sizeof(float) : 0;
+  return 1024 + STAGES * (BM * BK + BK * BN) * sizeof(T) + transposed + 2 * STAGES * sizeof(uint64_t);
+}
+
+// The GEMM kernel of each arithmetic type.
+using GemmKernel = void (*)(const CUtensorMap, const CUtensorMap, const SimtParams);
+template <typename T>
+GemmKernel gemm_kernel() {
+  if constexpr (std::is_same<T, float>::value) return simt_sgemm_kernel;
+  else return simt_gemm_kernel<T>;
 }
 
 template <typename T>
@@ -267,7 +431,7 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Si
   static bool attr_set = false;  // per process; the attribute is per function
   const size_t smem = smem_bytes<T>();
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(simt_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<T>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
@@ -277,7 +441,7 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Si
   } else {
     grid = dim3(p.tiles_n, p.tiles_m, p.splits);
   }
-  simt_gemm_kernel<T><<<grid, kThreads, smem, stream>>>(tmA, tmB, p);
+  gemm_kernel<T>()<<<grid, kThreads, smem, stream>>>(tmA, tmB, p);
   return cudaGetLastError();
 }
 
@@ -306,9 +470,9 @@ cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, 
 template <typename T>
 int occupancy() {
   const size_t smem = smem_bytes<T>();
-  cudaFuncSetAttribute(simt_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(gemm_kernel<T>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, simt_gemm_kernel<T>, kThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gemm_kernel<T>(), kThreads, smem) != cudaSuccess)
     return 0;
   return blocks;
 }
