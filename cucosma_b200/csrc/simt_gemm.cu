@@ -10,7 +10,8 @@
 //   * FP64 (simt_gemm_kernel<double>) reads 2 k-values of 8 rows per step
 //     straight from the swizzled tile; FP32 (simt_sgemm_kernel) first
 //     transposes each A stage into a k-major buffer, so a k-step is 4 LDS.128
-//     feeding 64 FFMA, and runs two CTAs per SM at 128 registers;
+//     feeding 32 two-lane FFMA2 (sm_100's packed FP32 FMA, each lane an
+//     fmaf), and runs two CTAs per SM at 128 registers;
 //   * 8 compute warps hold a 128x128 CTA tile, 8x8 outputs per thread;
 //   * split-K writes raw partial tiles to a caller-provided workspace and a
 //     separate kernel reduces them in ascending split order (deterministic),
@@ -224,11 +225,14 @@ __device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParam
   }
 }
 
-// FP32 kernel.  Same TMA/mbarrier ring as simt_gemm_kernel, but every A
-// stage is transposed once in shared memory into a k-major buffer (double
-// buffered, one CTA barrier per stage), so each k costs 2 LDS.128 for the 8 A
-// values and 2 for the 8 B values of a thread's 8x8 tile (thread rows are two
-// groups of 4 consecutive rows).  128 registers: two CTAs per SM.
+// FP32 kernel.  Same TMA ring as simt_gemm_kernel, but every A stage is
+// transposed once in shared memory into a k-major buffer (double buffered),
+// so each k costs 2 LDS.128 for the 8 A values and 2 for the 8 B values of a
+// thread's 8x8 tile (thread rows are two groups of 4 consecutive rows).  The
+// one CTA barrier per stage that publishes the transposed tile also proves
+// that every warp finished the previous stage, so thread 0 refills that
+// stage right after it: no empty barriers, no producer wait on the critical
+// path.  128 registers: two CTAs per SM.
 namespace simt {
 constexpr int kLdT = BM + 4;  // k-major A row pitch (floats): 16-byte aligned rows
 }
@@ -245,7 +249,6 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
   uint8_t* Bs = smem + STAGES * A_STAGE;
   float* AsT = reinterpret_cast<float*>(smem + STAGES * (A_STAGE + B_STAGE));  // [2][BK][kLdT]
   uint64_t* full = reinterpret_cast<uint64_t*>(AsT + 2 * BK * kLdT);
-  uint64_t* empty = full + STAGES;
 
   int tile_n, tile_m;  // block-index remap, cuCOSMAV100.cuh:2586-2603
   if (p.swizzle > 1) {
@@ -262,31 +265,26 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
   const int nkb = kend > kbeg ? (int)ceil_div(kend - kbeg, BK) : 0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kComputeWarps);
-    }
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
 
-  int issued = 0;
-  auto produce = [&](int kb) -> bool {
+  // Stage kb % STAGES is free: all reads of its previous use finished before
+  // a CTA barrier this thread has passed.
+  auto produce = [&](int kb) {
     const int s = kb % STAGES;
-    if (!mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1, kErrTimeoutEmpty, p.ctl)) return false;
     mbar_arrive_expect_tx(&full[s], A_STAGE + B_STAGE);
     const int kx = (int)(kbeg + (int64_t)kb * BK);
     tma_load_2d(As + s * A_STAGE, &tmA, kx, m0, &full[s]);
     tma_load_2d(Bs + s * B_STAGE, &tmB, n0, kx, &full[s]);
-    issued = kb + 1;
-    return true;
   };
-  bool ok = true;
   if (tid == 0) {
     tma_prefetch_desc(&tmA);
     tma_prefetch_desc(&tmB);
-    for (int kb = 0; kb < min(nkb, STAGES - 1) && ok; ++kb) ok = produce(kb);
+    for (int kb = 0; kb < min(nkb, STAGES - 1); ++kb) produce(kb);
   }
+  int issued = min(nkb, STAGES - 1);  // uniform across the CTA
 
   const int wm = warp >> 1, wn = warp & 1;
   const int tx = lane & 7, ty = lane >> 3;
@@ -294,24 +292,25 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
   const int b_col = wn * 64 + tx * 4;  // columns: b_col + {0..3}, b_col + 32 + {0..3}
   // transpose role: thread handles row tr, k-half th (8 consecutive k)
   const int tr = tid & (BM - 1), th = tid >> 7;
-  float acc[8][8];
+  const int sw = (tr >> 1) & 3;  // 64-byte TMA swizzle of row tr: chunk ^ ((tr >> 1) & 3)
+  const int c0 = ((2 * th) ^ sw) << 4, c1 = ((2 * th + 1) ^ sw) << 4;
+  // acc[i][q]: row i, columns 2q and 2q + 1 of the thread's 8 (packed pairs
+  // for the two-lane FFMA2 of sm_100: half the issue slots of scalar FFMA)
+  float2 acc[8][4];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
 
+  bool ok = true;
   for (int kb = 0; kb < nkb; ++kb) {
-    bool good = ok;
-    if (tid == 0 && good && kb + STAGES - 1 < nkb) good = produce(kb + STAGES - 1);
     const int s = kb % STAGES;
-    if (good) good = mbar_wait(&full[s], (kb / STAGES) & 1, kErrTimeoutFull, p.ctl);
+    const bool good = mbar_wait(&full[s], (kb / STAGES) & 1, kErrTimeoutFull, p.ctl);
     float* at = AsT + (kb & 1) * BK * kLdT;
     if (good) {
-      // two 16-byte chunks of row tr (64-byte swizzle: chunk ^ ((tr >> 1) & 3))
       const uint8_t* arow = As + s * A_STAGE + tr * 64;
-      const int sw = (tr >> 1) & 3;
-      const float4 q0 = *reinterpret_cast<const float4*>(arow + (((2 * th) ^ sw) << 4));
-      const float4 q1 = *reinterpret_cast<const float4*>(arow + (((2 * th + 1) ^ sw) << 4));
+      const float4 q0 = *reinterpret_cast<const float4*>(arow + c0);
+      const float4 q1 = *reinterpret_cast<const float4*>(arow + c1);
       float* col = at + th * 8 * kLdT + tr;
       col[0 * kLdT] = q0.x;
       col[1 * kLdT] = q0.y;
@@ -325,6 +324,11 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
     // Uniform across the CTA: nobody leaves the loop while others wait here.
     ok = __syncthreads_and(good);
     if (!ok) break;
+    // every warp is past stage kb - 1: refill its slot
+    if (kb + STAGES - 1 < nkb) {
+      if (tid == 0) produce(kb + STAGES - 1);
+      issued = kb + STAGES;
+    }
     const float* bs = reinterpret_cast<const float*>(Bs + s * B_STAGE);
 #pragma unroll
     for (int k = 0; k < BK; ++k) {
@@ -333,25 +337,35 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
       const float4 b0 = *reinterpret_cast<const float4*>(bs + k * BN + b_col);
       const float4 b1 = *reinterpret_cast<const float4*>(bs + k * BN + b_col + 32);
       const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      const float2 b[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                           make_float2(b1.z, b1.w)};
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 8; ++i) {
+        const float2 ai = make_float2(a[i], a[i]);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int q = 0; q < 4; ++q) acc[i][q] = __ffma2_rn(ai, b[q], acc[i][q]);  // = fmaf per lane
+      }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
   }
   if (!ok) {
+    // loads still in flight write into this CTA's shared memory: wait for them
     if (tid == 0)
       for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
         mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, kErrTimeoutDrain, p.ctl);
     return;
   }
   int rows[8];
+  float out[8][8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i) rows[i] = m0 + a_col + (i & 3) + (i >> 2) * 16;
-  simt_store<float>(acc, p, rows, n0 + b_col);
+  for (int i = 0; i < 8; ++i) {
+    rows[i] = m0 + a_col + (i & 3) + (i >> 2) * 16;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      out[i][2 * q] = acc[i][q].x;
+      out[i][2 * q + 1] = acc[i][q].y;
+    }
+  }
+  simt_store<float>(out, p, rows, n0 + b_col);
 }
 
 // Deterministic split-K reduction: C = epi(alpha * sum_z ws[z] + beta*C),
@@ -413,7 +427,7 @@ namespace simt {
 template <typename T>
 size_t smem_bytes() {
   constexpr int BK = Cfg<T>::BK;
-  // FP32 adds the double-buffered k-major copy of A
+  // FP32 adds the double-buffered k-major copy of A (and needs no empty barriers)
   constexpr size_t transposed = std::is_same<T, float>::value ? 2 * BK * kLdT * sizeof(float) : 0;
   return 1024 + STAGES * (BM * BK + BK * BN) * sizeof(T) + transposed + 2 * STAGES * sizeof(uint64_t);
 }
