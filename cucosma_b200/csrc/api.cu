@@ -172,7 +172,7 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
   constexpr int BK = simt::Cfg<T>::BK;
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   CUtensorMap tmA, tmB;
-  if (!encode_2d(&tmA, dt, sizeof(T), A, d->k, d->m, d->lda, BK, simt::BM, CU_TENSOR_MAP_SWIZZLE_64B))
+  if (!encode_2d(&tmA, dt, sizeof(T), A, d->k, d->m, d->lda, BK, simt::BM, simt::Cfg<T>::A_SWIZZLE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (!encode_2d(&tmB, dt, sizeof(T), B, d->n, d->k, d->ldb, simt::BN, BK, CU_TENSOR_MAP_SWIZZLE_NONE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;

@@ -1,18 +1,17 @@
-// simt_gemm.cu -- native FP32 (FFMA) and FP64 (DFMA) GEMM for sm_100a.
+// simt_gemm.cu -- native FP32 (FFMA2) and FP64 (DMMA) GEMM for sm_100a.
 //
 // Replaces the reference kernel cosmaSgemm_kernel (cuCOSMAV100.cuh:2505-2756)
 // and its split-K reduction (cosmaSplitKReduce.cuh:20-58) with a B200 design:
-//   * thread 0 streams A and B tiles with TMA into a 4-stage shared memory
-//     ring guarded by mbarriers (the reference double-buffers with
-//     __syncthreads and register-staged loads that transpose A on the way);
-//   * A tiles land row-major with the 64-byte TMA swizzle (conflict-free
-//     16-byte reads of any row);
-//   * FP64 (simt_gemm_kernel<double>) reads 2 k-values of 8 rows per step
-//     straight from the swizzled tile; FP32 (simt_sgemm_kernel) first
-//     transposes each A stage into a k-major buffer, so a k-step is 4 LDS.128
-//     feeding 32 two-lane FFMA2 (sm_100's packed FP32 FMA, each lane an
-//     fmaf), and runs two CTAs per SM at 128 registers;
-//   * 8 compute warps hold a 128x128 CTA tile, 8x8 outputs per thread;
+//   * thread 0 streams A and B tiles with TMA into a shared memory ring
+//     guarded by mbarriers (the reference double-buffers with __syncthreads
+//     and register-staged loads that transpose A on the way);
+//   * A tiles land row-major with a TMA swizzle (conflict-free reads);
+//   * FP32 (simt_sgemm_kernel) transposes each A stage into a k-major buffer,
+//     so a k-step is 4 LDS.128 feeding 32 two-lane FFMA2 (sm_100's packed
+//     FP32 FMA, each lane an fmaf), 8x8 outputs a thread, two CTAs per SM;
+//   * FP64 (simt_dgemm_kernel) runs on FP64 tensor-core MMAs with a 64x32
+//     warp tile;
+//   * 8 warps hold a 128x128 CTA tile;
 //   * split-K writes raw partial tiles to a caller-provided workspace and a
 //     separate kernel reduces them in ascending split order (deterministic),
 //     then applies alpha/beta and the epilogue, like cosmaSplitKReduce;
@@ -23,156 +22,6 @@
 #include "simt_gemm.cuh"
 
 namespace cucosma {
-
-template <typename T>
-__device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParams& p, const int (&rows)[8], int c0);
-
-template <typename T>
-__global__ void __launch_bounds__(simt::kThreads, simt::Cfg<T>::MIN_BLOCKS)
-    simt_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     const SimtParams p) {
-  using namespace simt;
-  constexpr int BK = Cfg<T>::BK;
-  constexpr int VEC = Vec<T>::n;
-  using V = typename Vec<T>::type;
-  // A fragments cover KV = 2 consecutive k per row (an 8-byte load for FP32,
-  // 16-byte for FP64): 2 * (8 + 8) fragment registers, so FP32 fits 128
-  // registers and two CTAs per SM.
-  constexpr int KV = 2;
-  using AV = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-  constexpr int A_STAGE = BM * BK * (int)sizeof(T);
-  constexpr int B_STAGE = BK * BN * (int)sizeof(T);
-  constexpr int KG = BK / KV;  // k-groups per stage
-  static_assert(BK * sizeof(T) == 64, "A rows are 64 bytes (64-byte swizzle span)");
-
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* As = smem;
-  uint8_t* Bs = smem + STAGES * A_STAGE;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * (A_STAGE + B_STAGE));
-  uint64_t* empty = full + STAGES;
-
-  // Block-index remap (reference semantics, cuCOSMAV100.cuh:2586-2603).
-  int tile_n, tile_m;
-  if (p.swizzle > 1) {
-    tile_n = blockIdx.x / p.swizzle;
-    tile_m = blockIdx.y * p.swizzle + blockIdx.x % p.swizzle;
-    if (tile_m >= p.tiles_m) return;
-  } else {
-    tile_n = blockIdx.x;
-    tile_m = blockIdx.y;
-  }
-  const int m0 = tile_m * BM, n0 = tile_n * BN;
-  const int64_t kbeg = (int64_t)blockIdx.z * p.kchunk;
-  const int64_t kend = min((int64_t)p.k, kbeg + p.kchunk);
-  const int nkb = kend > kbeg ? (int)ceil_div(kend - kbeg, BK) : 0;
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kComputeWarps);
-    }
-    fence_mbar_init();
-  }
-  __syncthreads();
-
-  // Producer role (thread 0): load k-block kb into stage kb % STAGES once all
-  // warps released that stage.  Returns false if the wait for it expired.
-  int issued = 0;
-  auto produce = [&](int kb) -> bool {
-    const int s = kb % STAGES;
-    const uint32_t ph = (kb / STAGES) & 1;
-    if (!mbar_wait(&empty[s], ph ^ 1, kErrTimeoutEmpty, p.ctl)) return false;
-    mbar_arrive_expect_tx(&full[s], A_STAGE + B_STAGE);
-    const int kx = (int)(kbeg + (int64_t)kb * BK);
-    tma_load_2d(As + s * A_STAGE, &tmA, kx, m0, &full[s]);
-    tma_load_2d(Bs + s * B_STAGE, &tmB, n0, kx, &full[s]);
-    issued = kb + 1;
-    return true;
-  };
-  bool ok = true;
-  if (threadIdx.x == 0) {
-    tma_prefetch_desc(&tmA);
-    tma_prefetch_desc(&tmB);
-    for (int kb = 0; kb < min(nkb, STAGES - 1) && ok; ++kb) ok = produce(kb);
-  }
-
-  // ---------------------------------------------------------------- compute
-  const int wm = warp >> 1, wn = warp & 1;  // 4 x 2 warps, warp tile 32 x 64
-  const int tx = lane & 7, ty = lane >> 3;  // 8 x 4 threads
-  T acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
-
-  // This thread's A rows are r_i = wm*32 + ty + 4i (64-byte rows, byte
-  // offset a_base + 256 i); the 64-byte swizzle XORs the 16-byte chunk index
-  // with (r_i >> 1) & 3, which is sw0 for even i and sw0 ^ 2 for odd i.
-  const int a_base = (wm * 32 + ty) * 64;
-  const int sw0 = (ty >> 1) & 3;
-  constexpr int NJ = 8 / VEC;  // vectors per thread along N
-  const int b_col = wn * 64 + tx * VEC;
-
-  for (int kb = 0; kb < nkb && ok; ++kb) {
-    if (threadIdx.x == 0 && kb + STAGES - 1 < nkb) ok = produce(kb + STAGES - 1);
-    const int s = kb % STAGES;
-    if (!mbar_wait(&full[s], (kb / STAGES) & 1, kErrTimeoutFull, p.ctl)) {
-      ok = false;
-      break;
-    }
-    const uint8_t* as = As + s * A_STAGE;
-    const T* bs = reinterpret_cast<const T*>(Bs + s * B_STAGE);
-#pragma unroll
-    for (int kg = 0; kg < KG; ++kg) {
-      // KV consecutive k of 8 A rows (one 8- or 16-byte load each) and the
-      // 8 B columns of those k: KV * 64 FMAs.
-      const int kb_off = kg * KV * (int)sizeof(T);  // byte offset of k-group kg inside a 64-byte row
-      T a[8][KV];
-      T b[KV][8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int sw = (i & 1) ? (sw0 ^ 2) : sw0;
-        const AV v = *reinterpret_cast<const AV*>(as + a_base + 256 * i + ((((kb_off >> 4) ^ sw) << 4) | (kb_off & 15)));
-        const T* pv = reinterpret_cast<const T*>(&v);
-#pragma unroll
-        for (int e = 0; e < KV; ++e) a[i][e] = pv[e];
-      }
-#pragma unroll
-      for (int kk = 0; kk < KV; ++kk) {
-#pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-          const V v = *reinterpret_cast<const V*>(bs + (kg * KV + kk) * BN + b_col + j * 8 * VEC);
-          const T* pv = reinterpret_cast<const T*>(&v);
-#pragma unroll
-          for (int e = 0; e < VEC; ++e) b[kk][j * VEC + e] = pv[e];
-        }
-      }
-#pragma unroll
-      for (int kk = 0; kk < KV; ++kk)
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-#pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i][kk], b[kk][j], acc[i][j]);
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
-  }
-  if (!ok) {
-    // A wait expired.  Thread 0 drains (bounded) every load it issued that
-    // may still be in flight, so no copy targets this CTA after it exits.
-    if (threadIdx.x == 0)
-      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
-        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, kErrTimeoutDrain, p.ctl);
-    return;
-  }
-
-  int rows[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) rows[i] = m0 + wm * 32 + ty + 4 * i;
-  simt_store<T>(acc, p, rows, n0 + b_col);
-}
 
 // Epilogue of the SIMT kernels: this thread's 8 x 8 accumulators, rows
 // rows[i], columns c0 + j*8*VEC + [0, VEC) for j < 8/VEC; either raw partial
@@ -225,8 +74,7 @@ __device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParam
   }
 }
 
-// FP32 kernel.  Same TMA ring as simt_gemm_kernel, but every A stage is
-// transposed once in shared memory into a k-major buffer (double buffered),
+// FP32 kernel.  A TMA ring of 4 stages; every A stage is transposed once in shared memory into a k-major buffer (double buffered),
 // so each k costs 2 LDS.128 for the 8 A values and 2 for the 8 B values of a
 // thread's 8x8 tile (thread rows are two groups of 4 consecutive rows).  The
 // one CTA barrier per stage that publishes the transposed tile also proves
@@ -368,6 +216,171 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
   simt_store<float>(out, p, rows, n0 + b_col);
 }
 
+// FP64 kernel on the FP64 tensor-core MMA (mma.sync m16n8k8 .f64, the
+// DMMA path: same peak as DFMA on B200, but one instruction does 32 FMAs a
+// lane, so fragment loads and issue slots stop mattering).  8 warps in a 2x4
+// grid, warp tile 64x32 = 4x4 MMA tiles, 64 FP64 accumulators a thread.  A
+// stages (128 rows x 16 k, 128-byte rows) land with the 128-byte TMA swizzle;
+// B stages (16 k x 128 n) unswizzled.  Thread 0 refills a stage two stages
+// after it was consumed, so its wait on the stage's empty barrier rarely
+// blocks.
+namespace simt {
+constexpr int kDStages = 5;
+}
+
+__device__ __forceinline__ void dmma_m16n8k8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// out[r][c], out[r][c + 1] from the raw sums v0, v1 (partial) or
+// epi(alpha * v + beta * C) (final).  c is even and rows are 16-byte aligned.
+__device__ __forceinline__ void store_pair(const SimtParams& p, int r, int c, double v0, double v1) {
+  if (r >= p.m || c >= p.n) return;
+  const bool both = c + 1 < p.n;
+  if (p.partial) {
+    double* w = reinterpret_cast<double*>(p.out) + (int64_t)blockIdx.z * p.ws_split_stride + (int64_t)r * p.ldo + c;
+    if (both) *reinterpret_cast<double2*>(w) = make_double2(v0, v1);
+    else w[0] = v0;
+    return;
+  }
+  double* o = reinterpret_cast<double*>(p.out) + (int64_t)r * p.ldo + c;
+  if (both) {
+    double2 cv = make_double2(0.0, 0.0);
+    if (p.beta != 0.0) cv = *reinterpret_cast<const double2*>(o);
+    *reinterpret_cast<double2*>(o) = make_double2(apply_epi(combine(v0, p.alpha, p.beta, &cv.x), p.epilogue),
+                                                  apply_epi(combine(v1, p.alpha, p.beta, &cv.y), p.epilogue));
+  } else {
+    o[0] = apply_epi(combine(v0, p.alpha, p.beta, o), p.epilogue);
+  }
+}
+
+__global__ void __launch_bounds__(simt::kThreads, 1)
+    simt_dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const SimtParams p) {
+  using namespace simt;
+  constexpr int BK = Cfg<double>::BK;  // 16
+  constexpr int S = kDStages;
+  constexpr int A_STAGE = BM * BK * 8, B_STAGE = BK * BN * 8;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* As = smem;
+  uint8_t* Bs = smem + S * A_STAGE;
+  uint64_t* full = reinterpret_cast<uint64_t*>(Bs + S * B_STAGE);
+  uint64_t* empty = full + S;
+
+  int tile_n, tile_m;  // block-index remap, cuCOSMAV100.cuh:2586-2603
+  if (p.swizzle > 1) {
+    tile_n = blockIdx.x / p.swizzle;
+    tile_m = blockIdx.y * p.swizzle + blockIdx.x % p.swizzle;
+    if (tile_m >= p.tiles_m) return;
+  } else {
+    tile_n = blockIdx.x;
+    tile_m = blockIdx.y;
+  }
+  const int m0 = tile_m * BM, n0 = tile_n * BN;
+  const int64_t kbeg = (int64_t)blockIdx.z * p.kchunk;
+  const int64_t kend = min((int64_t)p.k, kbeg + p.kchunk);
+  const int nkb = kend > kbeg ? (int)ceil_div(kend - kbeg, BK) : 0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kComputeWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  int issued = 0;
+  auto produce = [&](int kb) -> bool {
+    const int s = kb % S;
+    if (!mbar_wait(&empty[s], ((kb / S) & 1) ^ 1, kErrTimeoutEmpty, p.ctl)) return false;
+    mbar_arrive_expect_tx(&full[s], A_STAGE + B_STAGE);
+    const int kx = (int)(kbeg + (int64_t)kb * BK);
+    tma_load_2d(As + s * A_STAGE, &tmA, kx, m0, &full[s]);
+    tma_load_2d(Bs + s * B_STAGE, &tmB, n0, kx, &full[s]);
+    issued = kb + 1;
+    return true;
+  };
+  bool ok = true;
+  if (tid == 0) {
+    tma_prefetch_desc(&tmA);
+    tma_prefetch_desc(&tmB);
+    for (int kb = 0; kb < min(nkb, S - 2) && ok; ++kb) ok = produce(kb);
+  }
+
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp >> 2, wn = warp & 3;
+  // A element (r, k) of a stage sits at r * 128 + (((k >> 1) ^ (r & 7)) << 4) + (k & 1) * 8;
+  // every row this thread reads has r & 7 == g.
+  const uint8_t* a_rows = As + (wm * 64 + g) * 128 + (t & 1) * 8;
+  int a_off[2][2];  // [k-step][k = t or t + 4]
+#pragma unroll
+  for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) a_off[ks][h] = ((((ks * 8 + t + 4 * h) >> 1) ^ g) << 4);
+  const uint8_t* b_cols = Bs + t * BN * 8 + (wn * 32 + g) * 8;
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+  for (int kb = 0; kb < nkb && ok; ++kb) {
+    if (tid == 0 && kb + S - 2 < nkb) ok = produce(kb + S - 2);
+    const int s = kb % S;
+    if (ok) ok = mbar_wait(&full[s], (kb / S) & 1, kErrTimeoutFull, p.ctl);
+    if (!ok) break;
+    const uint8_t* as = a_rows + s * A_STAGE;
+    const uint8_t* bs = b_cols + s * B_STAGE;
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+      double af[4][4], bf[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const uint8_t* r0 = as + mt * 16 * 128;
+        af[mt][0] = *reinterpret_cast<const double*>(r0 + a_off[ks][0]);
+        af[mt][1] = *reinterpret_cast<const double*>(r0 + 8 * 128 + a_off[ks][0]);
+        af[mt][2] = *reinterpret_cast<const double*>(r0 + a_off[ks][1]);
+        af[mt][3] = *reinterpret_cast<const double*>(r0 + 8 * 128 + a_off[ks][1]);
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const uint8_t* c0 = bs + (ks * 8) * BN * 8 + nt * 64;
+        bf[nt][0] = *reinterpret_cast<const double*>(c0);
+        bf[nt][1] = *reinterpret_cast<const double*>(c0 + 4 * BN * 8);
+      }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma_m16n8k8(acc[mt][nt], af[mt], bf[nt]);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok) {
+    // One warp's failure does not stop the others (no CTA barrier in the
+    // loop); each returns after its own failed wait, thread 0 after draining.
+    if (tid == 0)
+      for (int kb = max(0, issued - S); kb < issued; ++kb)
+        mbar_wait(&full[kb % S], (kb / S) & 1, kErrTimeoutDrain, p.ctl);
+    return;
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        store_pair(p, m0 + wm * 64 + mt * 16 + g + 8 * h, n0 + wn * 32 + nt * 8 + 2 * t, acc[mt][nt][2 * h],
+                   acc[mt][nt][2 * h + 1]);
+}
+
 // Deterministic split-K reduction: C = epi(alpha * sum_z ws[z] + beta*C),
 // z ascending, the sum accumulated in T (cosmaSplitKReduce.cuh:31-40).
 template <typename T>
@@ -429,7 +442,8 @@ size_t smem_bytes() {
   constexpr int BK = Cfg<T>::BK;
   // FP32 adds the double-buffered k-major copy of A (and needs no empty barriers)
   constexpr size_t transposed = std::is_same<T, float>::value ? 2 * BK * kLdT * sizeof(float) : 0;
-  return 1024 + STAGES * (BM * BK + BK * BN) * sizeof(T) + transposed + 2 * STAGES * sizeof(uint64_t);
+  constexpr int stages = std::is_same<T, float>::value ? STAGES : kDStages;
+  return 1024 + stages * (BM * BK + BK * BN) * sizeof(T) + transposed + 2 * stages * sizeof(uint64_t);
 }
 
 // The GEMM kernel of each arithmetic type.
@@ -437,7 +451,7 @@ using GemmKernel = void (*)(const CUtensorMap, const CUtensorMap, const SimtPara
 template <typename T>
 GemmKernel gemm_kernel() {
   if constexpr (std::is_same<T, float>::value) return simt_sgemm_kernel;
-  else return simt_gemm_kernel<T>;
+  else return simt_dgemm_kernel;
 }
 
 template <typename T>

@@ -36,13 +36,13 @@ template <typename T>
 struct Cfg;
 template <>
 struct Cfg<float> {
-  static constexpr int BK = 16;         // 64-byte A rows
-  static constexpr int MIN_BLOCKS = 2;  // 128 registers: two CTAs (16 warps) per SM
+  static constexpr int BK = 16;  // 64-byte A rows
+  static constexpr CUtensorMapSwizzle A_SWIZZLE = CU_TENSOR_MAP_SWIZZLE_64B;
 };
 template <>
 struct Cfg<double> {
-  static constexpr int BK = 8;
-  static constexpr int MIN_BLOCKS = 1;  // 8x8 FP64 accumulators alone take 128 registers
+  static constexpr int BK = 16;  // 128-byte A rows
+  static constexpr CUtensorMapSwizzle A_SWIZZLE = CU_TENSOR_MAP_SWIZZLE_128B;
 };
 
 template <typename T>
