@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) grouped_ozaki_exp_kernel(const GroupEntry
   }
 }
 
-// Ozaki slices of every problem (packed layout): blocks [0, a_blocks) take
+// Ozaki slices of every problem (A packed, B stacked): blocks [0, a_blocks) take
 // 8 rows of some A (warp per row, lanes over 4-column groups); the rest take
 // one 32 (k) x 32 (n) tile of some B, transposed.
 template <int S>
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEnt
       int8_t q[S];
       slice_value<S>(tile[lane][i], e.eb[n], q);
 #pragma unroll
-      for (int s = 0; s < S; ++s) out[packed_index<S>(n, k, e.kpad, s)] = q[s];
+      for (int s = 0; s < S; ++s) out[stacked_index<S>(n, k, e.n, s)] = q[s];
     }
   }
 }
@@ -232,7 +232,7 @@ cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr
     L.kind = 2;
     L.slices = d->slices ? d->slices : kOzakiDefaultSlices;
     if (L.slices < 4 || L.slices > 9) return CUCOSMA_STATUS_NOT_SUPPORTED;
-    L.bn = L.slices <= 8 ? 64 : 48;
+    L.bn = ozaki_bn(L.slices);
   } else if (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6) {
     if (d->dtype != CUCOSMA_R_32F) return CUCOSMA_STATUS_NOT_SUPPORTED;
     L.kind = d->precision == CUCOSMA_PRECISION_BF16X6 ? 1 : 0;
@@ -350,8 +350,8 @@ extern "C" cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d
       const uint64_t kbs = (uint64_t)e.kpad / 32;
       ok = encode_3d(&e.tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e.planes_a, 32ull * s_, kbs, e.m, 32ull * s_,
                      (uint64_t)e.kpad * s_, 128, 1, 128, CU_TENSOR_MAP_SWIZZLE_128B) &&
-           encode_3d(&e.tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e.planes_b, 32ull * s_, kbs, e.n, 32ull * s_,
-                     (uint64_t)e.kpad * s_, 128, 1, L.bn, CU_TENSOR_MAP_SWIZZLE_128B);
+           encode_3d(&e.tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, e.planes_b, 32, e.n, kbs * s_, 32, 32ull * e.n, 32,
+                     ozaki_sub(s_), s_, CU_TENSOR_MAP_SWIZZLE_32B);
     } else {
       ok = encode_3d(&e.tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, e.planes_a, e.k, e.m, s_, e.kpad,
                      (uint64_t)e.m * e.kpad, 32, 128, s_, CU_TENSOR_MAP_SWIZZLE_64B) &&

@@ -9,8 +9,8 @@
 // Ozaki slicing (INT8 DGEMM): per row of A / per column of B the exponent
 // e with |x| < 2^e over the row / column; x * 2^-e is cut into s signed
 // 7-bit integer slices q_t = trunc(r * 2^7), r <- r * 2^7 - q_t, exact in
-// FP64.  Slices of A rows and of B columns (B transposed) are stored packed
-// (see packed_index), kpad = K rounded up to the 32-wide k-block.
+// FP64.  Slices of A rows are stored packed (packed_index), those of B
+// columns stacked (stacked_index); kpad = K rounded up to the 32-wide k-block.
 //
 // All pre-passes are HBM-bound elementwise / transpose kernels.
 #include <cuda_bf16.h>
@@ -184,7 +184,7 @@ __global__ void ozaki_slice_rows_kernel(const double* __restrict__ A, int64_t ld
   }
 }
 
-// B (K x N) -> packed slices of its columns, through a 32 x 32 tile
+// B (K x N) -> stacked slices of its columns, through a 32 x 32 tile
 // (32 x 8 threads); a tile row covers one k-block.
 template <int S>
 __global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
@@ -202,7 +202,7 @@ __global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ld
       int8_t q[S];
       slice_value<S>(tile[threadIdx.x][i], eb[n], q);
 #pragma unroll
-      for (int t = 0; t < S; ++t) out[packed_index<S>(n, k, kpad, t)] = q[t];
+      for (int t = 0; t < S; ++t) out[stacked_index<S>(n, k, ncols, t)] = q[t];
     }
   }
 }

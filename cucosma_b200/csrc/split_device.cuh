@@ -55,6 +55,13 @@ template <int S>
 __device__ __forceinline__ int64_t packed_index(int64_t r, int k, int64_t kpad, int p) {
   return r * (kpad * S) + (int64_t)(k >> 5) * (32 * S) + p * 32 + (k & 31);
 }
+// Stacked layout of the B slices: [k-block][slice][column][32 bytes of K],
+// so one TMA box brings all slices of a run of columns as a K-major matrix
+// whose rows are (slice, column) -- the B operand of the stacked-N MMAs.
+template <int S>
+__device__ __forceinline__ int64_t stacked_index(int64_t n, int k, int64_t ncols, int p) {
+  return ((int64_t)(k >> 5) * S + p) * (ncols * 32) + n * 32 + (k & 31);
+}
 
 // Backward-pass source transforms of the BF16 split (see SplitXform).
 template <int MODE>

@@ -44,7 +44,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
   if (d->precision == CUCOSMA_PRECISION_OZAKI) {
     pl.kind = 2;
     pl.slices = d->slices ? d->slices : kOzakiDefaultSlices;
-    pl.bn = pl.slices <= 8 ? 64 : (pl.slices <= 10 ? 48 : 32);
+    pl.bn = ozaki_bn(pl.slices);
     pl.bk = 32;
     pl.kpad = round_up(K, 32);
   } else {
@@ -203,12 +203,13 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
                               di->sms, st);
     launches += 4;
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
-    // Packed slices as a 3-D byte tensor {32 s (slices of one k-block), k-blocks, rows}.
+    // A slices (packed) as a 3-D byte tensor {32 s (slices of one k-block), k-blocks, rows}; B slices
+    // (stacked) as {32 bytes, columns, k-block * s + slice}, one box = all slices of a sub-tile.
     const uint64_t kbs = (uint64_t)pl.kpad / 32;
     if (!encode_3d(&ta, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_a, 32ull * s, kbs, m, 32ull * s,
                    (uint64_t)pl.kpad * s, 128, 1, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_b, 32ull * s, kbs, n, 32ull * s,
-                   (uint64_t)pl.kpad * s, 128, 1, pl.bn, CU_TENSOR_MAP_SWIZZLE_128B))
+        !encode_3d(&tb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, w + pl.off_b, 32, n, kbs * s, 32, 32ull * n, 32, ozaki_sub(s),
+                   s, CU_TENSOR_MAP_SWIZZLE_32B))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     p.ea = ea;
     p.eb = eb;

@@ -8,6 +8,15 @@ namespace cucosma {
 
 constexpr int kOzakiDefaultSlices = 8;
 
+// Ozaki tile geometry for S slices (stacked form, see tc_kernel.cuh): the B
+// slices of a sub-tile of ozaki_sub(S) output columns are stacked along N, so
+// one MMA of N = (S - p) * sub columns covers every diagonal that A slice p
+// feeds; S * sub <= 256 (the largest MMA N).  ozaki_nsub(S) sub-tiles fill
+// the 512 TMEM columns; the tile is 128 x ozaki_bn(S).
+constexpr int ozaki_sub(int s) { return s <= 4 ? 64 : (s == 5 ? 48 : (s <= 8 ? 32 : 16)); }
+constexpr int ozaki_nsub(int s) { return 512 / (s * ozaki_sub(s)); }
+constexpr int ozaki_bn(int s) { return ozaki_nsub(s) * ozaki_sub(s); }
+
 namespace tc {
 
 // One problem of a grouped launch, stored in the workspace.  The tensor maps

@@ -154,6 +154,26 @@ __device__ __forceinline__ void issue_terms(std::integer_sequence<int, Ts...>, u
   (issue_term<Tr, Ts>(ad0, bd0, acc0, not_first_kb), ...);
 }
 
+// Stacked Ozaki form: for sub-tile J and A slice P, one MMA of N = (S - P) *
+// SUB columns whose B operand is the stacked slices 0 .. S-1-P of the
+// sub-tile (rows (q, column)), accumulating A_P * B_q into the diagonal
+// block d = P + q at TMEM column (J * S + P + q) * SUB.  P = 0 spans every
+// diagonal, so on a unit's first k-block it initialises the accumulators
+// (accumulate = 0) before the narrower MMAs of P > 0 add to them.
+template <class Tr, int J, int P>
+__device__ __forceinline__ void issue_stacked_one(uint64_t ad0, uint32_t b_base, uint32_t acc0, bool not_first_kb) {
+  constexpr int S = Tr::NA, SUB = Tr::SUB;
+  constexpr uint32_t IDESC = idesc_s8_s32(128, (S - P) * SUB);
+  const uint64_t ad = ad0 + (uint64_t)(Tr::a_off(P, 0) >> 4);
+  const uint64_t bd = sdesc<32>(b_base + (uint32_t)(J * Tr::B_SUB_BYTES));
+  mma_i8(acc0 + (uint32_t)((J * S + P) * SUB), ad, bd, IDESC, P > 0 || not_first_kb);
+}
+template <class Tr, int... Is>
+__device__ __forceinline__ void issue_stacked(std::integer_sequence<int, Is...>, uint64_t ad0, uint32_t b_base,
+                                              uint32_t acc0, bool not_first_kb) {
+  (issue_stacked_one<Tr, Is / Tr::NA, Is % Tr::NA>(ad0, b_base, acc0, not_first_kb), ...);
+}
+
 template <class Tr>
 __global__ void __launch_bounds__(Tr::THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
@@ -229,9 +249,16 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
             // boxes of [rows][128 B]: slices 4j..4j+3 of k-block kb
 #pragma unroll
             for (int j = 0; j < Tr::TILES_A; ++j) tma_load_3d(st + j * Tr::A_TILE, u.ta, j * 128, kb, tm * 128, &full[s]);
+            if constexpr (Tr::STACKED) {
+              // per sub-tile one box [slices][SUB columns][32 B] of k-block kb
 #pragma unroll
-            for (int j = 0; j < Tr::TILES_B; ++j)
-              tma_load_3d(st + A_REGION + j * Tr::B_TILE, u.tb, j * 128, kb, tn * BN, &full[s]);
+              for (int j = 0; j < Tr::NSUB; ++j)
+                tma_load_3d(st + A_REGION + j * Tr::B_SUB_BYTES, u.tb, 0, tn * BN + j * Tr::SUB, kb * NB, &full[s]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < Tr::TILES_B; ++j)
+                tma_load_3d(st + A_REGION + j * Tr::B_TILE, u.tb, j * 128, kb, tn * BN, &full[s]);
+            }
           } else {
             // one box of [planes][rows][BK] per operand
             tma_load_3d(st, u.ta, kb * Tr::BK, tm * 128, 0, &full[s]);
@@ -269,8 +296,13 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
             tc_fence_after();
             const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
             const uint64_t ad0 = sdesc<SWZ>(a_base);
-            const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
-            issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != cs);
+            if constexpr (Tr::STACKED) {
+              issue_stacked<Tr>(std::make_integer_sequence<int, Tr::NSUB * NA>{}, ad0, a_base + A_REGION, acc0,
+                                kb != cs);
+            } else {
+              const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
+              issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != cs);
+            }
             mma_commit(&empty[s]);  // stage free once these MMAs have read it
           }
           if (!ok) break;
@@ -433,8 +465,9 @@ struct EpiF32 {
 
 // FP64 result (Ozaki).  Chunks of 16 columns: part = sum_{d = S-1..0}
 // S_d * 2^(-7(d+2)) (FP64, d descending), then 2^(e_row + e_col) and
-// alpha/beta; or the raw part into the split-K workspace.
-template <int S>
+// alpha/beta; or the raw part into the split-K workspace.  Accumulator
+// layout: sub-tiles of SUB columns, each S diagonal blocks of SUB columns.
+template <int S, int SUB>
 struct EpiOzaki {
   static constexpr int STAGING_PER_WARP = 32 * 17 * 8;
   template <int BN>
@@ -449,7 +482,7 @@ struct EpiOzaki {
 #pragma unroll
       for (int d = S - 1; d >= 0; --d) {
         uint32_t v[16];
-        tmem_ld16(tacc + d * BN + c0, v);
+        tmem_ld16(tacc + (uint32_t)((c0 / SUB) * S * SUB + d * SUB + c0 % SUB), v);
         tmem_ld_wait();
         const double w = ldexp(1.0, -7 * (d + 2));
 #pragma unroll
@@ -492,10 +525,17 @@ constexpr int kSmemBudget = 227 * 1024;
 // 128-byte swizzled row, so slice p sits in tile p / 4 at byte offset
 // (p % 4) * 32 -- selected like a K offset inside the swizzle atom.
 template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi, bool PROMOTE_ = false,
-          int CHUNK_ = 0, int EPI_WARPS_ = 4>
+          int CHUNK_ = 0, int EPI_WARPS_ = 4, int SUB_ = 0>
 struct TraitsBase {
   static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
   static constexpr bool kInt8 = INT8_;
+  // SUB > 0: stacked Ozaki form -- B slices of each SUB-column sub-tile
+  // stacked along N (one [NB][SUB][32 B] box, 32-byte swizzle), NSUB
+  // sub-tiles per tile, NACC = NB diagonal blocks per sub-tile.
+  static constexpr int SUB = SUB_;
+  static constexpr bool STACKED = SUB_ > 0;
+  static constexpr int NSUB = STACKED ? BN_ / SUB_ : 1;
+  static constexpr int B_SUB_BYTES = STACKED ? NB_ * SUB_ * 32 : 0;
   static constexpr bool PROMOTE = PROMOTE_;
   static constexpr int CHUNK = CHUNK_;
   // 4 epilogue warps (one per TMEM lane quadrant) or 8 (each quadrant
@@ -521,7 +561,10 @@ struct TraitsBase {
       PROMOTE ? (512 / (NACC * BN) > 4 ? 4 : 512 / (NACC * BN)) : ((2 * NACC * BN <= 512) ? 2 : 1);
   static constexpr int STAGING_PER_WARP = Epi::STAGING_PER_WARP;
   static constexpr int STAGING_BYTES = EPI_WARPS * STAGING_PER_WARP;
-  static constexpr int STAGE_BYTES = TILES_A * A_TILE + TILES_B * B_TILE;
+  static constexpr int STAGE_BYTES = TILES_A * A_TILE + (STACKED ? NSUB * B_SUB_BYTES : TILES_B * B_TILE);
+  static_assert(!STACKED || (INT8_ && NSUB * SUB_ == BN_ && NB_ * SUB_ <= 256 && SUB_ % 16 == 0 &&
+                             B_SUB_BYTES % 256 == 0 && NACC_ == NB_),
+                "stacked form: INT8, whole sub-tiles, MMA N <= 256");
   static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
   static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
   static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
@@ -584,12 +627,16 @@ struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChu
       {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
-// Ozaki with S slices: all pairs (p, q) with p + q < S, ordered by p then q;
-// accumulator d = p + q (the first writer of diagonal d is (0, d)); BN chosen
-// so that S accumulators fit in TMEM.
+// Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into
+// diagonal d = p + q.  Stacked form: S MMAs per sub-tile and k-block (one
+// per A slice, N shrinking with p) instead of S(S+1)/2 narrow ones -- an MMA
+// instruction has a fixed cost in the tensor pipe's front end and reads its
+// whole A operand, so few wide MMAs keep the tensor cores busy.  (The term
+// table below describes the pairs; the stacked issue order is p ascending
+// within each sub-tile.)
 template <int S>
 struct OzakiBN {
-  static constexpr int value = S <= 8 ? 64 : (S <= 10 ? 48 : 32);
+  static constexpr int value = ozaki_bn(S);
 };
 template <int S>
 constexpr TermTable<S*(S + 1) / 2> ozaki_terms() {
@@ -606,7 +653,8 @@ constexpr TermTable<S*(S + 1) / 2> ozaki_terms() {
   return t;
 }
 template <int S>
-struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, EpiOzaki<S>> {
+struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, EpiOzaki<S, ozaki_sub(S)>, false, 0,
+                          4, ozaki_sub(S)> {
   static constexpr TermTable<S*(S + 1) / 2> kTerms = ozaki_terms<S>();
 };
 

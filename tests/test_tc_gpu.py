@@ -154,11 +154,16 @@ def test_ozaki_slices_bitexact(dist):
     g_ea = ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32)
     g_eb = ws[plan["off_eb"]: plan["off_eb"] + 4 * n].view(np.int32)
     def unpack(off, rows):
-        # packed layout: [rows][k-block][slice][32 bytes] -> [slice][rows][k]
+        # packed layout (A): [rows][k-block][slice][32 bytes] -> [slice][rows][k]
         raw = ws[off: off + s * rows * kpad].view(np.int8).reshape(rows, kpad // 32, s, 32)
         return raw.transpose(2, 0, 1, 3).reshape(s, rows, kpad)
 
-    g_sa, g_sb = unpack(plan["off_a"], m), unpack(plan["off_b"], n)
+    def unstack(off, cols):
+        # stacked layout (B): [k-block][slice][cols][32 bytes] -> [slice][cols][k]
+        raw = ws[off: off + s * cols * kpad].view(np.int8).reshape(kpad // 32, s, cols, 32)
+        return raw.transpose(1, 2, 0, 3).reshape(s, cols, kpad)
+
+    g_sa, g_sb = unpack(plan["off_a"], m), unstack(plan["off_b"], n)
     assert np.array_equal(g_ea, ea) and np.array_equal(g_eb, eb)
     assert np.array_equal(g_sa[:, :, :k], sa) and np.array_equal(g_sb[:, :, :k], sb)
     assert not g_sa[:, :, k:].any() and not g_sb[:, :, k:].any()  # K padding is zero
@@ -229,3 +234,27 @@ def test_plan_reports_launches():
         cc.gemm(A, B, Cm, precision=prec)
         torch.cuda.synchronize()
         assert cc.launch_count() - n0 == plan["launches"]
+
+
+def test_ozaki_repeatable_and_exact_large():
+    """Stacked-N MMAs of different widths accumulate into overlapping TMEM
+    columns; repeated calls must agree bit for bit, and sampled rows must
+    match the restatement exactly (1024 x 1536 x 4096, 8 slices, 128 k-blocks
+    per tile)."""
+    import torch
+
+    m, n, k = 1024, 1536, 4096
+    A = uniform(40, (m, k), np.float64)
+    B = uniform(41, (k, n), np.float64)
+    dA, dB = to_dev(A), to_dev(B)
+    outs = []
+    for _ in range(4):
+        dC = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+        cc.gemm(dA, dB, dC, 1.0, 0.0, precision="ozaki", slices=8)
+        torch.cuda.synchronize()
+        outs.append(dC.cpu().numpy())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    idx = np.array([0, 1, 127, 128, 500, 777, 1023])
+    ref = oracle.ozaki_gemm(A[idx], B, 8)
+    assert np.array_equal(outs[0][idx], ref)
