@@ -41,6 +41,20 @@ METRIC = "TFLOP/s & % of peak: BF16x3/Ozaki vs native S/DGEMM at stated error vs
 OZAKI_SLICES = 8
 
 
+def dram_traffic(path, n):
+    """DRAM bytes (read + write) per launch of the path's main kernel at n^3, from
+    the ncu capture recorded in profiles/dram_traffic.txt; None if not captured."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
+            for line in f:
+                t = line.split()
+                if len(t) >= 5 and not t[0].startswith("#") and t[0] == path and int(t[1]) == n:
+                    return int(t[3]) + int(t[4])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -555,7 +569,8 @@ def main():
     kern_ms = hr.get("kernel_ms") or hr["ms"]
     achieved = flop / (kern_ms * 1e-3) / 1e12
     roof = {"bound": "tensor" if not head.startswith("native") else "simt", "achieved": achieved,
-            "peak": hr["peak_tflops"], "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"], "traffic": None,
+            "peak": hr["peak_tflops"], "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"],
+            "traffic": dram_traffic(head, n),
             "peak_source": pk["source"] + ": " + hr["peak"], "kernel_ms": kern_ms}
     dtypes = {"bf16x3": "bf16x3->f32", "bf16x6": "bf16x6->f32", "native_f32": "f32", "ozaki": "i8x%d->f64" % hslices,
               "native_f64": "f64"}

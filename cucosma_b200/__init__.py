@@ -139,8 +139,11 @@ def _ld(t):
     return t.stride(0) if t.shape[0] > 1 else max(t.stride(0), t.shape[1])
 
 
+FLAG_TEST_SKIP_STAGE = 1 << 30  # CUCOSMA_FLAG_TEST_SKIP_STAGE: failure-path test hook
+
+
 def make_desc(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none", split_k=0, swizzle=0,
-              slices=0, tile=0):
+              slices=0, tile=0, flags=0):
     m, k = A.shape
     k2, n = B.shape
     if k != k2 or tuple(Cm.shape) != (m, n):
@@ -153,7 +156,7 @@ def make_desc(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none"
     d.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     d.epilogue = EPILOGUES[epilogue] if isinstance(epilogue, str) else int(epilogue)
     d.alpha, d.beta = float(alpha), float(beta)
-    d.split_k, d.swizzle, d.slices, d.tile = int(split_k), int(swizzle), int(slices), int(tile)
+    d.split_k, d.swizzle, d.slices, d.tile, d.flags = int(split_k), int(swizzle), int(slices), int(tile), int(flags)
     return d
 
 
@@ -179,9 +182,9 @@ def alloc_workspace(desc, device=None):
 
 
 def gemm(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none", split_k=0, swizzle=0, slices=0,
-         tile=0, workspace=None, stream=None):
+         tile=0, workspace=None, stream=None, flags=0):
     """C <- epi(alpha*A@B + beta*C) in place on device tensors; returns C."""
-    d = make_desc(A, B, Cm, alpha, beta, precision, epilogue, split_k, swizzle, slices, tile)
+    d = make_desc(A, B, Cm, alpha, beta, precision, epilogue, split_k, swizzle, slices, tile, flags)
     if workspace is None:
         workspace = alloc_workspace(d, Cm.device)
     ws_ptr = workspace.data_ptr() if workspace is not None else None

@@ -110,7 +110,9 @@ cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B
   if (d->precision < CUCOSMA_PRECISION_NATIVE || d->precision > CUCOSMA_PRECISION_OZAKI)
     return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->epilogue < CUCOSMA_EPILOGUE_NONE || d->epilogue > CUCOSMA_EPILOGUE_RELU) return CUCOSMA_STATUS_INVALID_VALUE;
-  if (d->split_k < 0 || d->swizzle < 0 || d->flags != 0) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (d->split_k < 0 || d->swizzle < 0) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (d->flags != 0 && (d->flags != CUCOSMA_FLAG_TEST_SKIP_STAGE || d->precision == CUCOSMA_PRECISION_NATIVE))
+    return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->slices != 0 && (d->slices < 4 || d->slices > 12)) return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->m == 0 || d->n == 0) return CUCOSMA_STATUS_SUCCESS;
   if (d->ldc < d->n) return CUCOSMA_STATUS_INVALID_VALUE;

@@ -404,6 +404,7 @@ extern "C" cucosma_status cucosma_gemm_grouped(cucosma_grouped_plan plan, void* 
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TcParams p{};
+  p.skip_stage = -1;
   p.epilogue = plan->desc.epilogue;
   p.alpha = plan->desc.alpha;
   p.beta = plan->desc.beta;

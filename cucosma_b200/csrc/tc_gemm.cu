@@ -151,6 +151,7 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
   p.alpha = d->alpha;
   p.beta = d->beta;
   wait_ctl(di, &p.ctl.status, &p.ctl.timeout_ns);
+  p.skip_stage = (d->flags & CUCOSMA_FLAG_TEST_SKIP_STAGE) ? 0 : -1;
   if (pl.splits > 1) {
     p.partial = 1;
     p.out = w + pl.off_part;

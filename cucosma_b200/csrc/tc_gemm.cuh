@@ -57,6 +57,7 @@ struct TcParams {
   const int32_t* ea;  // Ozaki row exponents of A
   const int32_t* eb;  // Ozaki column exponents of B
   WaitCtl ctl;
+  int skip_stage;  // test hook: ring position whose loads the producer omits (-1: none)
   // Grouped launch: when ngroups > 0 the problems come from groups[] (all
   // other per-problem fields above are ignored) and units = total_tiles.
   const GroupEntry* groups;

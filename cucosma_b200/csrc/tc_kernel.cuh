@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
             break;
           }
           uint8_t* st = stages + s * STAGE_BYTES;
+          if (it == p.skip_stage) continue;  // test hook: this stage is never filled
           mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
           if constexpr (Tr::PACKED) {
             // boxes of [rows][128 B]: slices 4j..4j+3 of k-block kb

@@ -78,8 +78,17 @@ typedef struct cucosma_gemm_desc {
   int32_t split_k;        /* SPLIT_K: 0 = library/tuner choice, >= 1 forced */
   int32_t swizzle;        /* SWIZZLE: 0 = library choice, >= 1 forced block-index remap width */
   int32_t tile;           /* 0 = library/tuner choice, else a kernel configuration id */
-  int32_t flags;          /* reserved, must be 0 */
+  int32_t flags;          /* 0, or CUCOSMA_FLAG_TEST_SKIP_STAGE */
 } cucosma_gemm_desc;
+
+/* Test hook for the failure path (no counterpart in the reference, which
+ * exits the process on any CUDA error): on a tensor-core precision path the
+ * producer of every CTA leaves its first shared-memory stage unfilled, so the
+ * consumers' bounded waits expire; the call itself returns SUCCESS, the
+ * kernel stops early (C is left partly written) and cucosma_device_status
+ * then reports CUCOSMA_STATUS_TIMEOUT.  The CUDA context stays usable.  Pair
+ * it with a short cucosma_set_wait_timeout_ns. */
+#define CUCOSMA_FLAG_TEST_SKIP_STAGE (1 << 30)
 
 /* Fill *d with defaults: FP32, native, alpha = 1, beta = 0, no epilogue, auto split-K. */
 CUCOSMA_API void cucosma_gemm_desc_init(cucosma_gemm_desc* d);
