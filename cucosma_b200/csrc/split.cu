@@ -21,104 +21,119 @@
 namespace cucosma {
 
 // ------------------------------------------------------------------ BF16
-// A: rows x cols (ld elements) -> planes [nterms][rows][kpad], same layout.
-// Rows stride over grid.y, 4-column groups over grid.x (no 64-bit division
-// per element); each thread converts 4 consecutive columns (one 16-byte
-// load, one 8-byte store per plane).  Columns cols..kpad-1 are written as 0.
-template <int MODE>
-__global__ void split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
-                                       int nterms, __nv_bfloat16* __restrict__ out, const float* __restrict__ Y,
-                                       int64_t ldy, float scale) {
-  const int nc4 = (int)(kpad / 4);
+// Loads v[0..7] = src[c .. c+7] (zero past cols); c % 8 == 0 and src rows
+// 16-byte aligned, so the full case is two 16-byte loads.
+__device__ __forceinline__ void load8(const float* __restrict__ src, int c, int cols, float (&v)[8]) {
+  if (c + 8 <= cols) {
+    const float4 a = *reinterpret_cast<const float4*>(src + c);
+    const float4 b = *reinterpret_cast<const float4*>(src + c + 4);
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = c + e < cols ? src[c + e] : 0.f;
+  }
+}
+
+// A: rows x cols (ld elements) -> planes [NT][rows][kpad], same layout.
+// Rows stride over grid.y, 8-column groups over grid.x; each thread converts
+// 8 consecutive columns (two 16-byte loads, one 16-byte store per plane).
+// Columns cols..kpad-1 are written as 0 (kpad % 8 == 0).
+template <int MODE, int NT>
+__global__ void __launch_bounds__(256)
+    split_bf16_rows_kernel(const float* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
+                           __nv_bfloat16* __restrict__ out, const float* __restrict__ Y, int64_t ldy, float scale) {
+  const int ng = (int)(kpad / 8);
   const int64_t plane = (int64_t)rows * kpad;
   for (int r = blockIdx.y; r < rows; r += gridDim.y) {
     const float* srow = A + (int64_t)r * lda;
     __nv_bfloat16* drow = out + (int64_t)r * kpad;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nc4; g += gridDim.x * blockDim.x) {
-      const int c = g * 4;
-      float v[4];
-      if (c + 4 <= cols) {
-        const float4 q = *reinterpret_cast<const float4*>(srow + c);
-        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
-      } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) v[e] = c + e < cols ? srow[c + e] : 0.f;
-      }
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+      const int c = g * 8;
+      float v[8];
+      load8(srow, c, cols, v);
       if constexpr (MODE != kXformNone) {
-        const float* yrow = Y + (int64_t)r * ldy;
-        float y[4];
-        if (c + 4 <= cols) {
-          const float4 q = *reinterpret_cast<const float4*>(yrow + c);
-          y[0] = q.x, y[1] = q.y, y[2] = q.z, y[3] = q.w;
-        } else {
+        float y[8];
+        load8(Y + (int64_t)r * ldy, c, cols, y);
 #pragma unroll
-          for (int e = 0; e < 4; ++e) y[e] = c + e < cols ? yrow[c + e] : 0.f;
-        }
-#pragma unroll
-        for (int e = 0; e < 4; ++e) v[e] = xform<MODE>(v[e], y[e], scale);
+        for (int e = 0; e < 8; ++e) v[e] = xform<MODE>(v[e], y[e], scale);
       }
-      __nv_bfloat16 t[4][3];
+      uint32_t pk[NT][4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) split_bf16_value(v[e], nterms, t[e]);
-      for (int i = 0; i < nterms; ++i) {
-        uint2 pk;
-        pk.x = pack_bf16x2(t[0][i], t[1][i]);
-        pk.y = pack_bf16x2(t[2][i], t[3][i]);
-        *reinterpret_cast<uint2*>(drow + i * plane + c) = pk;  // kpad % 8 == 0: 8-byte aligned
+      for (int e = 0; e < 4; ++e) {
+        __nv_bfloat16 t0[NT], t1[NT];
+        split_bf16_n<NT>(v[2 * e], t0);
+        split_bf16_n<NT>(v[2 * e + 1], t1);
+#pragma unroll
+        for (int i = 0; i < NT; ++i) pk[i][e] = pack_bf16x2(t0[i], t1[i]);
       }
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        *reinterpret_cast<uint4*>(drow + i * plane + c) = make_uint4(pk[i][0], pk[i][1], pk[i][2], pk[i][3]);
     }
   }
 }
 
-// B: K x N (ld elements) -> planes [nterms][N][kpad] (transposed), through a
-// 64 (k) x 64 (n) shared-memory tile; block 32 x 8.  Loads are 256-byte
-// rows of B (float2 per lane); each lane stores two consecutive k of one
-// output row as a 4-byte pair, so a warp writes 128 contiguous bytes per
-// plane.
-template <int MODE>
-__global__ void split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
-                                       int nterms, __nv_bfloat16* __restrict__ out, const float* __restrict__ Y,
-                                       int64_t ldy, float scale) {
+// B: K x N (ld elements) -> planes [NT][N][kpad] (transposed), through a
+// 64 (k) x 64 (n) shared-memory tile; 256 threads.  Loads: 16 lanes cover a
+// 256-byte row of B (float4 each).  Stores: a lane converts 4 consecutive k
+// of one output row (8 bytes per plane), so 16 lanes write 128 contiguous
+// bytes per plane.
+template <int MODE, int NT>
+__global__ void __launch_bounds__(256)
+    split_bf16_cols_kernel(const float* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
+                           __nv_bfloat16* __restrict__ out, const float* __restrict__ Y, int64_t ldy, float scale) {
   __shared__ float tile[64][65];
   const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
   const int64_t plane = (int64_t)ncols * kpad;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;  // 16 x 16
 #pragma unroll
-  for (int i = ty; i < 64; i += 8) {
-    const int k = k0 + i, n = n0 + 2 * tx;
-    const float* src = B + (int64_t)k * ldb + n;
-    float2 v = make_float2(0.f, 0.f);
+  for (int i = ty; i < 64; i += 16) {
+    const int k = k0 + i, n = n0 + 4 * tx;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
     if (k < krows) {
-      if (n + 1 < ncols) {
-        v = *reinterpret_cast<const float2*>(src);  // n even, ldb % 4 == 0: 8-byte aligned
-      } else if (n < ncols) {
-        v.x = src[0];
+      const float* src = B + (int64_t)k * ldb + n;
+      if (n + 4 <= ncols) {
+        const float4 q = *reinterpret_cast<const float4*>(src);  // n % 4 == 0, ldb % 4 == 0
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[e] = n + e < ncols ? src[e] : 0.f;
       }
       if constexpr (MODE != kXformNone) {
         const float* ysrc = Y + (int64_t)k * ldy + n;
-        float2 y = make_float2(0.f, 0.f);
-        if (n + 1 < ncols)
-          y = *reinterpret_cast<const float2*>(ysrc);
-        else if (n < ncols)
-          y.x = ysrc[0];
-        v.x = xform<MODE>(v.x, y.x, scale);
-        v.y = xform<MODE>(v.y, y.y, scale);
+        float y[4] = {0.f, 0.f, 0.f, 0.f};
+        if (n + 4 <= ncols) {
+          const float4 q = *reinterpret_cast<const float4*>(ysrc);
+          y[0] = q.x, y[1] = q.y, y[2] = q.z, y[3] = q.w;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) y[e] = n + e < ncols ? ysrc[e] : 0.f;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[e] = xform<MODE>(v[e], y[e], scale);
       }
     }
-    tile[i][2 * tx] = v.x;
-    tile[i][2 * tx + 1] = v.y;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) tile[i][4 * tx + e] = v[e];
   }
   __syncthreads();
-  const int k = k0 + 2 * tx;
-#pragma unroll 2
-  for (int i = ty; i < 64; i += 8) {
+  const int k = k0 + 4 * tx;
+#pragma unroll
+  for (int i = ty; i < 64; i += 16) {
     const int n = n0 + i;
-    if (n < ncols && k < kpad) {  // kpad even, so k + 1 < kpad as well
-      __nv_bfloat16 t0[3], t1[3];
-      split_bf16_value(tile[2 * tx][i], nterms, t0);
-      split_bf16_value(tile[2 * tx + 1][i], nterms, t1);
+    if (n < ncols && k < kpad) {  // kpad % 8 == 0, so k + 3 < kpad as well
+      uint32_t pk[NT][2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        __nv_bfloat16 t0[NT], t1[NT];
+        split_bf16_n<NT>(tile[4 * tx + 2 * e][i], t0);
+        split_bf16_n<NT>(tile[4 * tx + 2 * e + 1][i], t1);
+#pragma unroll
+        for (int j = 0; j < NT; ++j) pk[j][e] = pack_bf16x2(t0[j], t1[j]);
+      }
       __nv_bfloat16* dst = out + (int64_t)n * kpad + k;
-      for (int j = 0; j < nterms; ++j) *reinterpret_cast<uint32_t*>(dst + j * plane) = pack_bf16x2(t0[j], t1[j]);
+#pragma unroll
+      for (int j = 0; j < NT; ++j) *reinterpret_cast<uint2*>(dst + j * plane) = make_uint2(pk[j][0], pk[j][1]);
     }
   }
 }
@@ -214,20 +229,28 @@ static unsigned grid_for(int64_t work, int threads, int sms) {
   return (unsigned)std::max<int64_t>(b, 1);
 }
 
-template <int MODE>
-static void split_bf16_launch(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
-                              bool transpose, int sms, cudaStream_t st, const float* Y, int64_t ldy, float scale) {
+template <int MODE, int NT>
+static void split_bf16_launch_nt(const float* A, int64_t lda, int rows, int cols, int64_t kpad, void* out,
+                                 bool transpose, int sms, cudaStream_t st, const float* Y, int64_t ldy, float scale) {
   if (!transpose) {
-    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(ceil_div(kpad / 4, 256), 16));
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(ceil_div(kpad / 8, 256), 16));
     const int64_t gy = std::max<int64_t>(1, std::min<int64_t>({(int64_t)rows, (int64_t)sms * 16 / gx, 65535}));
-    split_bf16_rows_kernel<MODE><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(
-        A, lda, rows, cols, kpad, nterms, static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
+    split_bf16_rows_kernel<MODE, NT><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(
+        A, lda, rows, cols, kpad, static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
   } else {
     // A is K x N here (krows = rows, ncols = cols); output N x kpad.
     dim3 grid((unsigned)ceil_div(cols, 64), (unsigned)ceil_div(kpad, 64));
-    split_bf16_cols_kernel<MODE><<<grid, dim3(32, 8), 0, st>>>(A, lda, rows, cols, kpad, nterms,
-                                                               static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
+    split_bf16_cols_kernel<MODE, NT><<<grid, 256, 0, st>>>(A, lda, rows, cols, kpad,
+                                                          static_cast<__nv_bfloat16*>(out), Y, ldy, scale);
   }
+}
+template <int MODE>
+static void split_bf16_launch(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,
+                              bool transpose, int sms, cudaStream_t st, const float* Y, int64_t ldy, float scale) {
+  if (nterms == 3)
+    split_bf16_launch_nt<MODE, 3>(A, lda, rows, cols, kpad, out, transpose, sms, st, Y, ldy, scale);
+  else
+    split_bf16_launch_nt<MODE, 2>(A, lda, rows, cols, kpad, out, transpose, sms, st, Y, ldy, scale);
 }
 
 cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, int64_t kpad, int nterms, void* out,

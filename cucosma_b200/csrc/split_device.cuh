@@ -19,6 +19,17 @@ __device__ __forceinline__ void split_bf16_value(float x, int nterms, __nv_bfloa
   }
 }
 
+// The same with the term count known at compile time (no local memory).
+template <int NT>
+__device__ __forceinline__ void split_bf16_n(float x, __nv_bfloat16 (&t)[NT]) {
+  float r = x;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    t[i] = __float2bfloat16_rn(r);
+    r = r - __bfloat162float(t[i]);
+  }
+}
+
 __device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
   __nv_bfloat162 v = __halves2bfloat162(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
