@@ -4,8 +4,8 @@ Workload (single GPU): the precision forms at M = N = K = 8192, alpha = 1,
 beta = 0, entries i.i.d. uniform[-1, 1] from fixed seeds (synthetic; the
 reference uses no dataset).  The headline "step" is one FP32 SGEMM through
 the BF16x3 tensor-core path (split pre-pass + tcgen05 GEMM); the same
-protocol times the native FP32 (FFMA) SGEMM, the native FP64 (DFMA) DGEMM
-and the Ozaki INT8-slice DGEMM, each reported with TFLOP/s, % of its
+protocol times the native FP32 (FFMA2) SGEMM, the native FP64 (FP64 tensor-core MMA)
+DGEMM and the Ozaki INT8-slice DGEMM, each reported with TFLOP/s, % of its
 relevant peak and its error against an FP64 (double-double for FP64 paths)
 CPU oracle evaluated on a sample of rows.
 
@@ -21,6 +21,12 @@ on all host threads.
 
 Multi-GPU: the path does not shard (one GEMM per GPU); --gpus N runs N
 independent replicas, one per rank, and reports the aggregate.
+
+--precision-sweep (not part of the driver contract) prints one JSON line per
+(size, value distribution, path): sizes 8192 and 16384, entries uniform[-1, 1]
+or sign * exp(N(0, sigma = 8)), paths native FP32, BF16x3, BF16x6, native FP64
+and Ozaki with 6..9 slices; TFLOP/s and the max / mean relative and normwise
+errors on 8 sampled rows against the FP64 (double-double for FP64 paths) oracle.
 """
 from __future__ import annotations
 
@@ -320,6 +326,60 @@ def grouped_bench(cc, precision, dtype, slices, steps, warmup, seed=5):
 
 
 # -------------------------------------------------------------- CPU legs
+def make_dist(n, seed, dist):
+    """FP64 device matrix: uniform[-1, 1], or sign * exp(X), X ~ N(0, 8^2)."""
+    import torch
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    if dist == "uniform":
+        return torch.rand((n, n), generator=g, device="cuda", dtype=torch.float64) * 2 - 1
+    sign = torch.where(torch.rand((n, n), generator=g, device="cuda", dtype=torch.float64) < 0.5, -1.0, 1.0)
+    return sign * torch.exp(8.0 * torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64))
+
+
+def precision_sweep(args):
+    """Precision forms at 8192^3 and 16384^3 on both value distributions."""
+    import torch
+
+    import cucosma_b200 as cc
+    import oracle
+
+    threads = oracle.lib().oracle_max_threads()
+    sizes = [int(x) for x in args.sweep_sizes.split(",")]
+    for n in sizes:
+        for dist in ("uniform", "expspread"):
+            A64, B64 = make_dist(n, 1, dist), make_dist(n, 2, dist)
+            idx = np.linspace(0, n - 1, 8).astype(np.int64)
+            A64h, B64h = A64.cpu().numpy(), B64.cpu().numpy()
+            A32, B32 = A64.float(), B64.float()
+            A32h, B32h = A32.cpu().numpy(), B32.cpu().numpy()
+            ref32 = oracle.gemm(A32h[idx], B32h, threads=threads)
+            hi, lo = oracle.gemm(A64h[idx], B64h, dd=True, threads=threads)
+            del A64h, B64h, A32h, B32h
+            paths = [("native_f32", "native", 0, A32, B32), ("bf16x3", "bf16x3", 0, A32, B32),
+                     ("bf16x6", "bf16x6", 0, A32, B32), ("native_f64", "native", 0, A64, B64)]
+            paths += [("ozaki_s%d" % s_, "ozaki", s_, A64, B64) for s_ in (6, 7, 8, 9)]
+            for name, prec, slices, A, B in paths:
+                Cm = torch.zeros((n, n), dtype=A.dtype, device="cuda")
+                d = cc.make_desc(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices)
+                ws = cc.alloc_workspace(d)
+                ms, kern_ms, _ = time_path(cc, A, B, Cm, prec, slices, args.steps, args.warmup, 1, ws)
+                out = Cm[torch.as_tensor(idx, device="cuda")].cpu().numpy()
+                err = oracle.errors(out, ref32) if A.dtype == torch.float32 else oracle.errors(out, hi, lo)
+                err["nonfinite"] = int((~np.isfinite(out)).sum())
+                print(json.dumps({"sweep": "precision", "n": n, "dist": dist, "path": name, "ms": ms,
+                                  "tflops": 2.0 * n ** 3 / (ms * 1e-3) / 1e12, "kernel_ms": kern_ms,
+                                  "error_vs_fp64": err}), flush=True)
+                del Cm, ws
+            del A64, B64, A32, B32
+            torch.cuda.empty_cache()
+    st, code = cc.device_status()
+    if st != cc.SUCCESS:
+        raise SystemExit("device status %d (detail 0x%x)" % (st, code))
+    return 0
+
+
 def cpu_sample(n, A32, B32, A64, B64, outs, budget_s=12.0):
     """CPU baseline leg: times the FP64 oracle on a bounded sample of rows of
     the FP32 workload (all host threads) and uses the same rows -- plus a
@@ -470,10 +530,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline / error leg")
     ap.add_argument("--only", default="", help="comma-separated subset of paths (profiling runs): "
                     "bf16x3,bf16x6,native_f32,ozaki,native_f64,grouped_bf16x3,grouped_ozaki,fwd_bwd")
+    ap.add_argument("--precision-sweep", action="store_true", help="precision forms x sizes x distributions")
+    ap.add_argument("--sweep-sizes", default="8192,16384")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.precision_sweep:
+        return precision_sweep(args)
 
     import torch
 
