@@ -16,6 +16,7 @@
 #include "../../include/cucosma.h"
 #include "api_internal.cuh"
 #include "simt_gemm.cuh"
+#include "skinny.cuh"
 
 namespace cucosma {
 
@@ -213,13 +214,31 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
   return CUCOSMA_STATUS_SUCCESS;
 }
 
+// Skinny-shape kernels (skinny.cu) for native precision: tiny K, or tiny M or N.
+static SkinnyPlan plan_skinny_for(const cucosma_gemm_desc* d, int sms) {
+  return plan_skinny(d->m, d->n, d->k, d->dtype == CUCOSMA_R_32F ? 4 : 8, d->split_k, d->tile, sms);
+}
+
+template <typename T>
+static cucosma_status run_skinny(const cucosma_gemm_desc* d, const SkinnyPlan& sp, const T* A, const T* B, T* C,
+                                 void* ws, const DeviceInfo* di, cudaStream_t st) {
+  prof_begin(st);
+  const cudaError_t e = launch_skinny<T>(sp, A, d->lda, B, d->ldb, C, d->ldc, (int)d->m, (int)d->n, (int)d->k,
+                                         d->alpha, d->beta, d->epilogue, ws, di->sms, st);
+  prof_end(st);
+  note_launches(sp.splits > 1 ? 2 : 1);
+  return e == cudaSuccess ? CUCOSMA_STATUS_SUCCESS : CUCOSMA_STATUS_LAUNCH_FAILED;
+}
+
 cucosma_status workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const DeviceInfo* di) {
   *bytes = 0;
   if (d->m == 0 || d->n == 0 || d->k == 0 || d->alpha == 0.0) return CUCOSMA_STATUS_SUCCESS;
   switch (d->precision) {
-    case CUCOSMA_PRECISION_NATIVE:
-      *bytes = plan_native(d, di->sms).ws_bytes;
+    case CUCOSMA_PRECISION_NATIVE: {
+      const SkinnyPlan sp = plan_skinny_for(d, di->sms);
+      *bytes = sp.kind ? sp.ws_bytes : plan_native(d, di->sms).ws_bytes;
       return CUCOSMA_STATUS_SUCCESS;
+    }
     default:
       return tc_workspace_size(d, bytes, di);
   }
@@ -250,6 +269,10 @@ cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, vo
   if (need > 0 && (ws == nullptr || ws_bytes < need)) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
   if (need > 0 && !aligned16(ws)) return CUCOSMA_STATUS_MISALIGNED;
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
+    const SkinnyPlan sp = plan_skinny_for(d, di->sms);
+    if (sp.kind)
+      return fp32 ? run_skinny<float>(d, sp, (const float*)A, (const float*)B, (float*)C, ws, di, st)
+                  : run_skinny<double>(d, sp, (const double*)A, (const double*)B, (double*)C, ws, di, st);
     const NativePlan pl = plan_native(d, di->sms);
     return fp32 ? run_native<float>(d, pl, (const float*)A, (const float*)B, (float*)C, ws, di, st)
                 : run_native<double>(d, pl, (const double*)A, (const double*)B, (double*)C, ws, di, st);
@@ -344,6 +367,21 @@ extern "C" cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cuco
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
   cucosma_gemm_desc tuned;
   d = apply_tuning(d, &tuned, di);
+  if (d->precision == CUCOSMA_PRECISION_NATIVE && plan_skinny_for(d, di->sms).kind) {
+    const SkinnyPlan sp = plan_skinny_for(d, di->sms);
+    info->path = 0;
+    info->tile_m = sp.tile_m;
+    info->tile_n = sp.tile_n;
+    info->tile_k = sp.kind == 1 ? (int32_t)d->k : 256;
+    info->splits = sp.splits;
+    info->band = 1;
+    info->slices = 1;
+    info->launches = sp.splits > 1 ? 2 : 1;
+    info->kchunk = sp.kind == 1 ? d->k : sp.kchunk;
+    info->kpad = d->k;
+    info->workspace_bytes = sp.ws_bytes;
+    return CUCOSMA_STATUS_SUCCESS;
+  }
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
     const NativePlan pl = plan_native(d, di->sms);
     info->path = 0;

@@ -399,8 +399,23 @@ __global__ void splitk_reduce_kernel(const T* __restrict__ ws, int64_t split_str
     if (c + VEC <= n) {
       V s = *reinterpret_cast<const V*>(w);
       T* ps = reinterpret_cast<T*>(&s);
-      for (int z = 1; z < splits; ++z) {
-        const V t = *reinterpret_cast<const V*>(w + z * split_stride);
+      // Splits are added in ascending order; the loads of a batch of 8 are
+      // issued before its adds so that many splits do not serialise on load
+      // latency.
+      int z = 1;
+      for (; z + 8 <= splits; z += 8) {
+        V t[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) t[j] = *reinterpret_cast<const V*>(w + (int64_t)(z + j) * split_stride);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const T* pt = reinterpret_cast<const T*>(&t[j]);
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) ps[e] += pt[e];
+        }
+      }
+      for (; z < splits; ++z) {
+        const V t = *reinterpret_cast<const V*>(w + (int64_t)z * split_stride);
         const T* pt = reinterpret_cast<const T*>(&t);
 #pragma unroll
         for (int e = 0; e < VEC; ++e) ps[e] += pt[e];
