@@ -138,10 +138,11 @@ cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B
 // --------------------------------------------------------------- planning
 static int simt_bk(int dtype) { return dtype == CUCOSMA_R_32F ? simt::Cfg<float>::BK : simt::Cfg<double>::BK; }
 
-NativePlan plan_native(const cucosma_gemm_desc* d, int sms) {
+NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws) {
   NativePlan p{};
+  const bool fp32 = d->dtype == CUCOSMA_R_32F;
   const int bk = simt_bk(d->dtype);
-  const int es = d->dtype == CUCOSMA_R_32F ? 4 : 8;
+  const int es = fp32 ? 4 : 8;
   const int vec = 16 / es;
   p.tiles_m = (int)ceil_div(d->m, simt::BM);
   p.tiles_n = (int)ceil_div(d->n, simt::BN);
@@ -150,9 +151,15 @@ NativePlan plan_native(const cucosma_gemm_desc* d, int sms) {
   int64_t splits = d->split_k;
   if (splits <= 0) {
     splits = 1;
-    if (tiles < sms) {
-      // Fill the machine (one CTA per SM) while keeping >= 32 k-blocks per split.
-      splits = std::max<int64_t>(1, std::min<int64_t>(sms / tiles, kblocks / 32));
+    // Resident CTA slots: two per SM for FP32 (128 registers), one for FP64.
+    const int64_t slots = (int64_t)sms * (fp32 ? simt::Cfg<float>::CTAS_PER_SM : simt::Cfg<double>::CTAS_PER_SM);
+    if (tiles < slots) {
+      // Fill one wave of slots (rounding down, so no partial second wave)
+      // while keeping >= 8 k-blocks per split; within max_ws.
+      splits = std::max<int64_t>(1, std::min<int64_t>(slots / tiles, kblocks / 8));
+      const size_t per_split = (size_t)d->m * (size_t)round_up(d->n, vec) * es;
+      if (splits > 1 && per_split > 0 && (size_t)splits * per_split > max_ws)
+        splits = std::max<int64_t>(1, (int64_t)(max_ws / per_split));
     }
   }
   splits = std::max<int64_t>(1, std::min<int64_t>(splits, kblocks));

@@ -24,7 +24,9 @@ struct NativePlan {
   int64_t kchunk, ldw;
   size_t ws_bytes;
 };
-NativePlan plan_native(const cucosma_gemm_desc* d, int sms);
+// Plan of the 128 x 128 tile kernel; an automatic split-K factor is chosen
+// so that its partial sums fit max_ws bytes.
+NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws = SIZE_MAX);
 
 cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B, const void* C);
 cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,

@@ -76,7 +76,7 @@ extern "C" cucosma_status cucosma_sgemm_splitk_static(int m, int n, int k, float
   const DeviceInfo* di = device_info();
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (di->cc_major != 10 || di->cc_minor != 0) return CUCOSMA_STATUS_ARCH_MISMATCH;
-  const NativePlan pl = plan_native(&d, di->sms);
+  const NativePlan pl = plan_native(&d, di->sms, (size_t)CUCOSMA_STATIC_SCRATCH_BYTES);
   if (pl.ws_bytes > (size_t)CUCOSMA_STATIC_SCRATCH_BYTES) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
   void* scratch = nullptr;
   if (pl.ws_bytes > 0) {

@@ -37,11 +37,13 @@ struct Cfg;
 template <>
 struct Cfg<float> {
   static constexpr int BK = 16;  // 64-byte A rows
+  static constexpr int CTAS_PER_SM = 2;
   static constexpr CUtensorMapSwizzle A_SWIZZLE = CU_TENSOR_MAP_SWIZZLE_64B;
 };
 template <>
 struct Cfg<double> {
   static constexpr int BK = 16;  // 128-byte A rows
+  static constexpr int CTAS_PER_SM = 1;
   static constexpr CUtensorMapSwizzle A_SWIZZLE = CU_TENSOR_MAP_SWIZZLE_128B;
 };
 

@@ -212,7 +212,8 @@ CUCOSMA_API cucosma_status cucosma_grouped_plan_destroy(cucosma_grouped_plan pla
  * cudaMalloc's implicit synchronisation.  Same arithmetic as cucosma_sgemm
  * with SPLIT_K = split_k (0 = library choice); the split-K partial sums live
  * in a fixed device array of CUCOSMA_STATIC_SCRATCH_BYTES inside the library,
- * held by every device that loads it until the process exits.  Problems whose
+ * held by every device that loads it until the process exits (the library's
+ * own split_k choice is capped to fit it).  Problems whose
  * partials (splits * m * round_up(n, 4) floats) exceed it return
  * CUCOSMA_STATUS_WORKSPACE_TOO_SMALL without launching.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress), so make
