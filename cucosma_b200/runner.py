@@ -8,7 +8,8 @@ row; the column order read by Kernel/cuda/run.sh:189: occupancy, TYPE,
 VECTORTYPE2, VECTORTYPE4, M, N, K, the tile sizes, SPLIT_K, ALPHA, BETA,
 SWIZZLE, A_OFFSET, B_OFFSET, ATOMIC_REDUCTION).  Every row runs as one GEMM
 through the C ABI (cucosma_gemm) with the row's M, N, K, TYPE, ALPHA, BETA,
-SPLIT_K and SWIZZLE; the tile and offset columns describe the reference
+SPLIT_K and SWIZZLE (or, with --library-schedule, the library's own split-K
+and swizzle); the tile and offset columns describe the reference
 kernel's compile-time tiling and are recorded, not used (this library picks
 its kernels at run time), and ATOMIC_REDUCTION is moot (the split-K reduction
 here is always deterministic).
@@ -131,6 +132,8 @@ def run_row(row, args, flush, gen_seed):
     C = pitched(m, n, dtype)
     C.copy_(C0)
     prec = args.precision
+    if args.library_schedule:
+        split_k = swizzle = 0
     kw = dict(precision=prec, split_k=split_k if split_k > 1 else 0, swizzle=swizzle if swizzle > 1 else 0)
     desc = cc.make_desc(A, B, C, alpha, beta, **kw)
     ws = cc.alloc_workspace(desc)
@@ -207,6 +210,8 @@ def main(argv=None):
     ap.add_argument("--check", action="store_true", help="check each result on sampled rows against FP64")
     ap.add_argument("--cublas", action="store_true", help="also time torch.matmul (cuBLAS, TF32 off)")
     ap.add_argument("--max-gb", type=float, default=40.0, help="skip rows whose A + B + C exceed this")
+    ap.add_argument("--library-schedule", action="store_true",
+                    help="ignore the rows' SPLIT_K and SWIZZLE (tuned for the reference's GPU) and let the library choose")
     args = ap.parse_args(argv)
 
     import torch
