@@ -168,10 +168,13 @@ __device__ __forceinline__ void issue_stacked_one(uint64_t ad0, uint32_t b_base,
   const uint64_t bd = sdesc<32>(b_base + (uint32_t)(J * Tr::B_SUB_BYTES));
   mma_i8(acc0 + (uint32_t)((J * S + P) * SUB), ad, bd, IDESC, P > 0 || not_first_kb);
 }
+// Issue order: A slice major (p = 0, 1, ...), sub-tiles inner, so the two
+// MMAs that read the same A slice are adjacent (measured 6 % faster than
+// sub-tile major); within each sub-tile p still ascends.
 template <class Tr, int... Is>
 __device__ __forceinline__ void issue_stacked(std::integer_sequence<int, Is...>, uint64_t ad0, uint32_t b_base,
                                               uint32_t acc0, bool not_first_kb) {
-  (issue_stacked_one<Tr, Is / Tr::NA, Is % Tr::NA>(ad0, b_base, acc0, not_first_kb), ...);
+  (issue_stacked_one<Tr, Is % Tr::NSUB, Is / Tr::NSUB>(ad0, b_base, acc0, not_first_kb), ...);
 }
 
 template <class Tr>
