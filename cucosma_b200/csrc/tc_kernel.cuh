@@ -626,9 +626,10 @@ struct Bf16x3Promoted : TraitsBase<3, 128, 64, 2, 2, 2, false, EpiF32, true, kPr
 // correction products accumulate in TMEM accumulator 1, the main product
 // hi*hi in accumulator 0, so the main accumulator is rounded only by its own
 // MMAs; both are promoted into FP32 registers every kPromoteChunk k-blocks.
+// Order: smallest first, MMAs that read the same A plane adjacent.
 struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk> {
   static constexpr TermTable<6> kTerms{
-      {2, 1, 0, 1, 0, 0}, {0, 1, 2, 0, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
+      {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
 // Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into
