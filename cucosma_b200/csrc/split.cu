@@ -139,85 +139,175 @@ __global__ void __launch_bounds__(256)
 }
 
 // ----------------------------------------------------------------- Ozaki
-// frexp-style exponent of the largest magnitude: |x| < 2^e for all x.
+// Column exponents of B start at this sentinel (a byte memset); columns that
+// are all zero keep it until ozaki_rows_kernel turns it into exp_of(0) = 0.
+constexpr int32_t kExpSentinel = (int32_t)0x80808080;
 
-// One warp per row of A.
-__global__ void ozaki_row_exp_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols,
-                                     int32_t* __restrict__ ea) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int r = warp; r < rows; r += nwarps) {
+// Column exponents of B (K x N): a block covers 64 rows of K and 512 columns
+// (two per thread, 16-byte loads).  Each block's column maxima enter eb by
+// atomicMax of their exponents -- exact, since the exponent of a maximum is
+// the maximum of the exponents (frexp is monotonic in |x|); zero maxima stay
+// out so that they cannot raise a column's exponent.
+__global__ void __launch_bounds__(256)
+    ozaki_col_exp_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int32_t* eb) {
+  const int c = (blockIdx.x * 256 + threadIdx.x) * 2;
+  const int k0 = blockIdx.y * 64, k1 = min(krows, k0 + 64);
+  if (c >= ncols) return;
+  double m0 = 0.0, m1 = 0.0;
+  if (c + 1 < ncols) {
+#pragma unroll 8
+    for (int k = k0; k < k1; ++k) {
+      const double2 v = *reinterpret_cast<const double2*>(B + (int64_t)k * ldb + c);  // c even, 16-byte rows
+      m0 = fmax(m0, fabs(v.x));
+      m1 = fmax(m1, fabs(v.y));
+    }
+  } else {
+    for (int k = k0; k < k1; ++k) m0 = fmax(m0, fabs(B[(int64_t)k * ldb + c]));
+  }
+  if (m0 != 0.0) atomicMax(&eb[c], exp_of(m0));
+  if (c + 1 < ncols && m1 != 0.0) atomicMax(&eb[c + 1], exp_of(m1));
+}
+
+// A rows -> row exponents and packed slices: a 256-thread block per row.
+// Rows of up to kRowRegK columns are read once into registers (4 consecutive
+// columns per thread and step, two 16-byte loads), the maximum is reduced
+// across the block, and the slices are cut from the registers; longer rows
+// take a second pass over the row for the slices.  A thread's 4 columns give
+// one 4-byte store per slice.  Also finishes B's column exponents
+// (sentinel -> 0).
+constexpr int kRowSteps = 8;                    // steps of 1024 columns held in registers
+constexpr int kRowRegK = kRowSteps * 1024;
+
+__device__ __forceinline__ void load4(const double* __restrict__ src, int c, int cols, double (&v)[4]) {
+  if (c + 4 <= cols) {
+    const double2 v0 = *reinterpret_cast<const double2*>(src + c);  // c % 4 == 0, 16-byte rows
+    const double2 v1 = *reinterpret_cast<const double2*>(src + c + 2);
+    v[0] = v0.x, v[1] = v0.y, v[2] = v1.x, v[3] = v1.y;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = c + j < cols ? src[c + j] : 0.0;
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void store_slices4(int8_t* __restrict__ out, int64_t r, int c, int64_t kpad,
+                                              const double (&v)[4], int e) {
+  int8_t q[4][S];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) slice_value<S>(v[j], e, q[j]);
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
+                        ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
+    *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, kpad, t)) = pk;
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256)
+    ozaki_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
+                      int32_t* __restrict__ ea, int8_t* __restrict__ out, int32_t* __restrict__ eb, int ncols) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncols; i += gridDim.x * blockDim.x)
+    if (eb[i] == kExpSentinel) eb[i] = 0;
+  __shared__ double red[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool in_regs = kpad <= kRowRegK;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    const double* src = A + (int64_t)r * lda;
+    double v[kRowSteps][4];
     double m = 0.0;
-    for (int c = lane; c < cols; c += 32) m = fmax(m, fabs(A[(int64_t)r * lda + c]));
+    if (in_regs) {
+#pragma unroll
+      for (int j = 0; j < kRowSteps; ++j) {
+        const int c = (tid + 256 * j) * 4;
+        if (c < kpad) {
+          load4(src, c, cols, v[j]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[j][q] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(v[j][q]));
+      }
+    } else {
+      for (int c = tid * 4; c < kpad; c += 1024) {
+        double w[4];
+        load4(src, c, cols, w);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(w[q]));
+      }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) ea[r] = exp_of(m);
+    if (lane == 0) red[warp] = m;
+    __syncthreads();
+    m = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmax(m, red[w]);
+    __syncthreads();  // red is reused by the next row
+    const int e = exp_of(m);
+    if (tid == 0) ea[r] = e;
+    if (in_regs) {
+#pragma unroll
+      for (int j = 0; j < kRowSteps; ++j) {
+        const int c = (tid + 256 * j) * 4;
+        if (c < kpad) store_slices4<S>(out, r, c, kpad, v[j], e);
+      }
+    } else {
+      for (int c = tid * 4; c < kpad; c += 1024) {
+        double w[4];
+        load4(src, c, cols, w);
+        store_slices4<S>(out, r, c, kpad, w, e);
+      }
+    }
   }
 }
 
-// Column maxima of B (K x N): block of 32 x 8 threads covers 32 columns,
-// the 8 thread rows stride over K.
-__global__ void ozaki_col_exp_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols,
-                                     int32_t* __restrict__ eb) {
-  __shared__ double red[8][33];
-  const int n = blockIdx.x * 32 + threadIdx.x;
-  double m = 0.0;
-  if (n < ncols)
-    for (int k = threadIdx.y; k < krows; k += 8) m = fmax(m, fabs(B[(int64_t)k * ldb + n]));
-  red[threadIdx.y][threadIdx.x] = m;
-  __syncthreads();
-  if (threadIdx.y == 0 && n < ncols) {
-    for (int i = 1; i < 8; ++i) m = fmax(m, red[i][threadIdx.x]);
-    eb[n] = exp_of(m);
-  }
-}
-
-
-// A rows -> packed slices; each thread slices 4 consecutive columns.
+// B (K x N) -> stacked slices of its columns, through a 32 (k) x 64 (n)
+// shared-memory tile.  Loads: 16 lanes cover 64 doubles of a row of B.
+// Stores: a lane slices 4 consecutive k of one column into one 4-byte store
+// per slice; 8 lanes cover a column's 32 bytes and a warp 4 adjacent columns
+// (128 contiguous bytes per slice).
 template <int S>
-__global__ void ozaki_slice_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
-                                        const int32_t* __restrict__ ea, int8_t* __restrict__ out) {
-  const int64_t c4 = kpad / 4;
-  const int64_t total = (int64_t)rows * c4;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = idx / c4;
-    const int c = (int)(idx - r * c4) * 4;
-    const int e = ea[r];
+__global__ void __launch_bounds__(256)
+    ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
+                            const int32_t* __restrict__ eb, int8_t* __restrict__ out) {
+  __shared__ double tile[32][65];
+  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 64, t = threadIdx.x;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int i = p * 16 + t / 16, c = (t % 16) * 4;
+    const int k = k0 + i, n = n0 + c;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (k < krows) {
+      const double* src = B + (int64_t)k * ldb + n;
+      if (n + 4 <= ncols) {
+        const double2 v0 = *reinterpret_cast<const double2*>(src);
+        const double2 v1 = *reinterpret_cast<const double2*>(src + 2);
+        v[0] = v0.x, v[1] = v0.y, v[2] = v1.x, v[3] = v1.y;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = n + j < ncols ? src[j] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tile[i][c + j] = v[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int item = p * 256 + t, nl = item / 8, kq = item % 8;
+    const int n = n0 + nl, k = k0 + kq * 4;
+    if (n >= ncols) continue;
+    const int e = eb[n];
     int8_t q[4][S];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double v = c + j < cols ? A[r * lda + c + j] : 0.0;
-      slice_value<S>(v, e, q[j]);
-    }
+    for (int j = 0; j < 4; ++j) slice_value<S>(tile[kq * 4 + j][nl], e, q[j]);
 #pragma unroll
-    for (int t = 0; t < S; ++t) {
-      const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
-                          ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
-      *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, kpad, t)) = pk;
-    }
-  }
-}
-
-// B (K x N) -> stacked slices of its columns, through a 32 x 32 tile
-// (32 x 8 threads); a tile row covers one k-block.
-template <int S>
-__global__ void ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
-                                        const int32_t* __restrict__ eb, int8_t* __restrict__ out) {
-  __shared__ double tile[32][33];
-  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int k = k0 + i, n = n0 + threadIdx.x;
-    tile[i][threadIdx.x] = (k < krows && n < ncols) ? B[(int64_t)k * ldb + n] : 0.0;
-  }
-  __syncthreads();
-  for (int i = threadIdx.y; i < 32; i += 8) {
-    const int n = n0 + i, k = k0 + threadIdx.x;
-    if (n < ncols && k < kpad) {
-      int8_t q[S];
-      slice_value<S>(tile[threadIdx.x][i], eb[n], q);
-#pragma unroll
-      for (int t = 0; t < S; ++t) out[stacked_index<S>(n, k, ncols, t)] = q[t];
+    for (int s_ = 0; s_ < S; ++s_) {
+      const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
+                          ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
+      *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, ncols, s_)) = pk;
     }
   }
 }
@@ -268,24 +358,30 @@ cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, i
 
 cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
                                    int32_t* ea, int32_t* eb, int sms, cudaStream_t st) {
-  ozaki_row_exp_kernel<<<grid_for((int64_t)m * 32, 256, sms), 256, 0, st>>>(A, lda, m, k, ea);
-  ozaki_col_exp_kernel<<<(unsigned)ceil_div(n, 32), dim3(32, 8), 0, st>>>(B, ldb, k, n, eb);
+  // Row exponents of A are found by ozaki_rows_kernel (launch_ozaki_slices).
+  (void)A, (void)lda, (void)m, (void)ea, (void)sms;
+  cudaError_t e = cudaMemsetAsync(eb, 0x80, (size_t)n * sizeof(int32_t), st);
+  if (e != cudaSuccess) return e;
+  if (k > 0) {
+    const dim3 grid((unsigned)ceil_div(n, 512), (unsigned)ceil_div(k, 64));
+    ozaki_col_exp_kernel<<<grid, 256, 0, st>>>(B, ldb, k, n, eb);
+  }
   return cudaGetLastError();
 }
 
 template <int S>
 static cudaError_t slices_s(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                            int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                            int64_t kpad, int32_t* ea, int32_t* eb, int8_t* sa, int8_t* sb, int sms,
                             cudaStream_t st) {
-  ozaki_slice_rows_kernel<S><<<grid_for((int64_t)m * (kpad / 4), 256, sms), 256, 0, st>>>(A, lda, m, k, kpad, ea,
-                                                                                           sa);
-  dim3 grid((unsigned)ceil_div(n, 32), (unsigned)ceil_div(kpad, 32));
-  ozaki_slice_cols_kernel<S><<<grid, dim3(32, 8), 0, st>>>(B, ldb, k, n, kpad, eb, sb);
+  const unsigned rows_grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(m, (int64_t)sms * 8));
+  ozaki_rows_kernel<S><<<rows_grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, eb, n);
+  dim3 grid((unsigned)ceil_div(n, 64), (unsigned)ceil_div(kpad, 32));
+  ozaki_slice_cols_kernel<S><<<grid, 256, 0, st>>>(B, ldb, k, n, kpad, eb, sb);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                                int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                                int64_t kpad, int32_t* ea, int32_t* eb, int8_t* sa, int8_t* sb, int sms,
                                 cudaStream_t st) {
   switch (s) {
     case 4: return slices_s<4>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);

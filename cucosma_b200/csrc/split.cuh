@@ -22,15 +22,18 @@ cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, i
                               bool transpose, int sms, cudaStream_t st, int xform = kXformNone,
                               const float* Y = nullptr, int64_t ldy = 0, float scale = 1.0f);
 
-// Per-row exponents of A (m x k) and per-column exponents of B (k x n).
+// Per-column exponents of B (k x n) into eb (the per-row exponents of A are
+// written by launch_ozaki_slices, which must follow on the same stream).
 cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
                                    int32_t* ea, int32_t* eb, int sms, cudaStream_t st);
 
-// s INT8 slices of the rows of A and of the columns of B, packed (four
-// slices' 32-byte k-blocks per 128-byte row): byte (r, k, p) at
-// r * kpad * s + (k / 32) * 32 * s + p * 32 + k % 32; kpad a multiple of 32.
+// Row exponents of A into ea, then s INT8 slices of the rows of A, packed
+// (four slices' 32-byte k-blocks per 128-byte row): byte (r, k, p) at
+// r * kpad * s + (k / 32) * 32 * s + p * 32 + k % 32; and of the columns of B,
+// stacked: byte (n, k, p) at ((k / 32) * s + p) * n_cols * 32 + n * 32 + k % 32.
+// kpad a multiple of 32.
 cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                                int64_t kpad, const int32_t* ea, const int32_t* eb, int8_t* sa, int8_t* sb, int sms,
+                                int64_t kpad, int32_t* ea, int32_t* eb, int8_t* sa, int8_t* sb, int sms,
                                 cudaStream_t st);
 
 }  // namespace cucosma

@@ -43,17 +43,33 @@ __device__ __forceinline__ int exp_of(double amax) {
   return e;
 }
 
-// Ozaki slices of one value scaled into (-1, 1): r <- r * 2^7, q = trunc(r),
-// r <- r - q; exact in FP64 (power-of-two scaling, integer part removal).
+// Ozaki slices of one value scaled into (-1, 1): the restatement's sequence
+// r <- v * 2^-e, then per slice r <- r * 2^7, q = trunc(r), r <- r - q is
+// exact in FP64, so q_t is the sign of v times the t-th 7-bit group of the
+// binary expansion of |v| * 2^-e.  Computed here from the bits of v with
+// integer operations (one 64-bit shift instead of 2 S FP64 conversions):
+// |v| = M * 2^(E - 1075) with the 53-bit significand M (E the biased
+// exponent; M without the hidden bit and E = 1 for subnormals), so the
+// first 7 S bits F = floor(|v| * 2^(7 S - e)) = M shifted by
+// 7 S - e + E - 1075 (right when negative).
 template <int S>
 __device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
-  double r = ldexp(v, -e);
+  static_assert(S * 7 <= 63, "slices exceed a 64-bit fixed-point value");
+  const uint64_t bits = (uint64_t)__double_as_longlong(v);
+  const int E = (int)((bits >> 52) & 0x7ff);
+  const uint64_t mant = bits & ((1ull << 52) - 1);
+  const uint64_t M = E ? (mant | (1ull << 52)) : mant;
+  const int sh = 7 * S - e + (E ? E : 1) - 1075;  // F = M * 2^sh
+  uint64_t F;
+  if (sh >= 0)
+    F = sh >= 64 ? 0 : (M << sh);  // |v| < 2^e bounds F below 2^(7 S)
+  else
+    F = -sh >= 64 ? 0 : (M >> -sh);
+  const bool neg = (bits >> 63) != 0;
 #pragma unroll
   for (int t = 0; t < S; ++t) {
-    r = r * 128.0;
-    const double w = trunc(r);
-    q[t] = (int8_t)(int)w;
-    r = r - w;
+    const int g = (int)((F >> (7 * (S - 1 - t))) & 127);
+    q[t] = (int8_t)(neg ? -g : g);
   }
 }
 

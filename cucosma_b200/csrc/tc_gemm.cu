@@ -116,7 +116,7 @@ void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan
   info->splits = pl.splits;
   info->band = pl.band;
   info->slices = pl.slices;
-  info->launches = (pl.kind == 2 ? 5 : 3) + (pl.splits > 1 ? 1 : 0);
+  info->launches = (pl.kind == 2 ? 4 : 3) + (pl.splits > 1 ? 1 : 0);
   info->kchunk = (int64_t)pl.kb_per_split * pl.bk;
   info->kpad = pl.kpad;
   info->workspace_bytes = pl.bytes;
@@ -204,7 +204,7 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
       e = launch_ozaki_slices(s, (const double*)A, d->lda, (const double*)B, d->ldb, m, n, k, pl.kpad, ea, eb,
                               reinterpret_cast<int8_t*>(w + pl.off_a), reinterpret_cast<int8_t*>(w + pl.off_b),
                               di->sms, st);
-    launches += 4;
+    launches += 3;
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
     // A slices (packed) as a 3-D byte tensor {32 s (slices of one k-block), k-blocks, rows}; B slices
     // (stacked) as {32 bytes, columns, k-block * s + slice}, one box = all slices of a sub-tile.

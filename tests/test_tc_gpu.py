@@ -258,3 +258,21 @@ def test_ozaki_repeatable_and_exact_large():
     idx = np.array([0, 1, 127, 128, 500, 777, 1023])
     ref = oracle.ozaki_gemm(A[idx], B, 8)
     assert np.array_equal(outs[0][idx], ref)
+
+
+def test_ozaki_zero_rows_and_columns():
+    """All-zero rows of A and columns of B take exponent 0 (the column
+    exponents are found by atomic maxima that zeros do not join); result and
+    exponents bit-exact vs the restatement."""
+    m, n, k, s = 70, 90, 300, 8
+    A = uniform(30, (m, k), np.float64)
+    B = uniform(31, (k, n), np.float64) * 1e-3
+    A[[0, 17, 69], :] = 0.0
+    B[:, [0, 5, 89]] = 0.0
+    B[:150, 40] = 0.0  # a column whose maximum lies in the second half of K
+    Cin = np.zeros((m, n))
+    out, plan, ws = run(A, B, Cin, 1.0, 0.0, "ozaki", slices=s, keep_ws=True)
+    ea, eb, _, _ = oracle.ozaki_slices(A, B, s)
+    assert np.array_equal(ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32), ea)
+    assert np.array_equal(ws[plan["off_eb"]: plan["off_eb"] + 4 * n].view(np.int32), eb)
+    assert np.array_equal(out, oracle.ozaki_gemm(A, B, s))
