@@ -11,6 +11,7 @@
 // The GEMM kernel numbers the tiles of all problems consecutively and each
 // CTA walks them round-robin (tc_kernel.cuh, resolve_unit), so small problems
 // no longer leave most of the GPU idle the way one launch per problem does.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -251,9 +252,15 @@ cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr
   L.off_b.resize(count);
   L.off_ea.resize(count);
   L.off_eb.resize(count);
+  // Table order: K descending (stable).  The persistent kernel hands units out
+  // round-robin in table order, so the long-K tiles are spread over the CTAs
+  // first and the short ones even out the end.
+  std::vector<int> order(count);
+  for (int i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pr[a].k > pr[b].k; });
   int tiles = 0, pa = 0, pb = 0, xa = 0, xb = 0;
   for (int i = 0; i < count; ++i) {
-    const cucosma_gemm_problem& q = pr[i];
+    const cucosma_gemm_problem& q = pr[order[i]];
     if (q.m <= 0 || q.n <= 0 || q.k <= 0) return CUCOSMA_STATUS_INVALID_VALUE;
     if (q.m > INT32_MAX || q.n > INT32_MAX || q.k > INT32_MAX) return CUCOSMA_STATUS_INVALID_VALUE;
     if (q.lda < q.k || q.ldb < q.n || q.ldc < q.n || !q.A || !q.B || !q.C) return CUCOSMA_STATUS_INVALID_VALUE;
