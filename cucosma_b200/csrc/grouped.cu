@@ -48,11 +48,14 @@ __device__ __forceinline__ int find_entry(const GroupEntry* g, int count, int b)
   return lo;
 }
 
-// BF16 split of every problem.  Blocks [0, a_blocks): 8 rows of some A per
-// block, one warp per row, lanes over 4-column groups.  Blocks after that:
-// one 64 (k) x 64 (n) tile of some B, transposed (as split_bf16_cols_kernel).
+// BF16 split of every problem (NT terms).  Blocks [0, a_blocks): 8 rows of
+// some A per block, one warp per row, lanes over 8-column groups (two 16-byte
+// loads, one 16-byte store per plane).  Blocks after that: one 64 (k) x 64 (n)
+// tile of some B, transposed: 16 lanes load 64 floats of a row; a lane then
+// converts 4 consecutive k of one column (one 8-byte store per plane).
+template <int NT>
 __global__ void __launch_bounds__(256) grouped_split_bf16_kernel(const GroupEntry* __restrict__ g, int count,
-                                                                 int a_blocks, int nterms) {
+                                                                 int a_blocks) {
   __shared__ float tile[64][65];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int b = blockIdx.x;
@@ -63,26 +66,30 @@ __global__ void __launch_bounds__(256) grouped_split_bf16_kernel(const GroupEntr
     const float* src = static_cast<const float*>(e.A) + (int64_t)r * e.lda;
     __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(e.planes_a) + (int64_t)r * e.kpad;
     const int64_t plane = (int64_t)e.m * e.kpad;
-    const int nc4 = (int)(e.kpad / 4);
-    for (int gi = lane; gi < nc4; gi += 32) {
-      const int c = gi * 4;
-      float v[4];
-      if (c + 4 <= e.k) {
-        const float4 q = *reinterpret_cast<const float4*>(src + c);
-        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    const int nc8 = (int)(e.kpad / 8);
+    for (int gi = lane; gi < nc8; gi += 32) {
+      const int c = gi * 8;
+      float v[8];
+      if (c + 8 <= e.k) {
+        const float4 q0 = *reinterpret_cast<const float4*>(src + c);  // 16-byte rows, c % 8 == 0
+        const float4 q1 = *reinterpret_cast<const float4*>(src + c + 4);
+        v[0] = q0.x, v[1] = q0.y, v[2] = q0.z, v[3] = q0.w, v[4] = q1.x, v[5] = q1.y, v[6] = q1.z, v[7] = q1.w;
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = c + j < e.k ? src[c + j] : 0.f;
+        for (int j = 0; j < 8; ++j) v[j] = c + j < e.k ? src[c + j] : 0.f;
       }
-      __nv_bfloat16 t[4][3];
+      uint32_t pk[NT][4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) split_bf16_value(v[j], nterms, t[j]);
-      for (int i = 0; i < nterms; ++i) {
-        uint2 pk;
-        pk.x = pack_bf16x2(t[0][i], t[1][i]);
-        pk.y = pack_bf16x2(t[2][i], t[3][i]);
-        *reinterpret_cast<uint2*>(dst + i * plane + c) = pk;
+      for (int j = 0; j < 4; ++j) {
+        __nv_bfloat16 t0[NT], t1[NT];
+        split_bf16_n<NT>(v[2 * j], t0);
+        split_bf16_n<NT>(v[2 * j + 1], t1);
+#pragma unroll
+        for (int i = 0; i < NT; ++i) pk[i][j] = pack_bf16x2(t0[i], t1[i]);
       }
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        *reinterpret_cast<uint4*>(dst + i * plane + c) = make_uint4(pk[i][0], pk[i][1], pk[i][2], pk[i][3]);
     }
     return;
   }
@@ -92,33 +99,44 @@ __global__ void __launch_bounds__(256) grouped_split_bf16_kernel(const GroupEntr
   const int tiles_n64 = (e.n + 63) / 64;
   const int k0 = (t / tiles_n64) * 64, n0 = (t % tiles_n64) * 64;
   const float* B = static_cast<const float*>(e.B);
-  const int tx = lane, ty = warp;
 #pragma unroll
-  for (int i = ty; i < 64; i += 8) {
-    const int k = k0 + i, n = n0 + 2 * tx;
-    const float* src = B + (int64_t)k * e.ldb + n;
-    float2 v = make_float2(0.f, 0.f);
+  for (int p = 0; p < 4; ++p) {
+    const int i = p * 16 + tid / 16, c = (tid % 16) * 4;
+    const int k = k0 + i, n = n0 + c;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
     if (k < e.k) {
-      if (n + 1 < e.n)
-        v = *reinterpret_cast<const float2*>(src);
-      else if (n < e.n)
-        v.x = src[0];
+      const float* src = B + (int64_t)k * e.ldb + n;
+      if (n + 4 <= e.n) {
+        const float4 q = *reinterpret_cast<const float4*>(src);  // n % 4 == 0, 16-byte rows
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = n + j < e.n ? src[j] : 0.f;
+      }
     }
-    tile[i][2 * tx] = v.x;
-    tile[i][2 * tx + 1] = v.y;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tile[i][c + j] = v[j];
   }
   __syncthreads();
   const int64_t plane = (int64_t)e.n * e.kpad;
-  const int k = k0 + 2 * tx;
   __nv_bfloat16* out = static_cast<__nv_bfloat16*>(e.planes_b);
-  for (int i = ty; i < 64; i += 8) {
-    const int n = n0 + i;
-    if (n < e.n && k < e.kpad) {
-      __nv_bfloat16 t0[3], t1[3];
-      split_bf16_value(tile[2 * tx][i], nterms, t0);
-      split_bf16_value(tile[2 * tx + 1][i], nterms, t1);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int item = p * 256 + tid, nl = item / 16, kq = item % 16;
+    const int n = n0 + nl, k = k0 + kq * 4;
+    if (n < e.n && k < e.kpad) {  // kpad % 8 == 0: k + 3 < kpad as well
+      uint32_t pk[NT][2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        __nv_bfloat16 t0[NT], t1[NT];
+        split_bf16_n<NT>(tile[kq * 4 + 2 * j][nl], t0);
+        split_bf16_n<NT>(tile[kq * 4 + 2 * j + 1][nl], t1);
+#pragma unroll
+        for (int i = 0; i < NT; ++i) pk[i][j] = pack_bf16x2(t0[i], t1[i]);
+      }
       __nv_bfloat16* dst = out + (int64_t)n * e.kpad + k;
-      for (int j = 0; j < nterms; ++j) *reinterpret_cast<uint32_t*>(dst + j * plane) = pack_bf16x2(t0[j], t1[j]);
+#pragma unroll
+      for (int i = 0; i < NT; ++i) *reinterpret_cast<uint2*>(dst + i * plane) = make_uint2(pk[i][0], pk[i][1]);
     }
   }
 }
@@ -425,8 +443,11 @@ extern "C" cucosma_status cucosma_gemm_grouped(cucosma_grouped_plan plan, void* 
   std::memset(&dummy, 0, sizeof(dummy));
   cudaError_t e;
   if (plan->kind != 2) {
-    grouped_split_bf16_kernel<<<plan->pre_a_blocks + plan->pre_b_blocks, 256, 0, st>>>(
-        plan->table, plan->count, plan->pre_a_blocks, plan->slices);
+    const unsigned blocks = (unsigned)(plan->pre_a_blocks + plan->pre_b_blocks);
+    if (plan->slices == 3)
+      grouped_split_bf16_kernel<3><<<blocks, 256, 0, st>>>(plan->table, plan->count, plan->pre_a_blocks);
+    else
+      grouped_split_bf16_kernel<2><<<blocks, 256, 0, st>>>(plan->table, plan->count, plan->pre_a_blocks);
     e = cudaGetLastError();
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
     prof_begin(st);
