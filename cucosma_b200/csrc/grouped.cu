@@ -178,11 +178,11 @@ __global__ void __launch_bounds__(256) grouped_ozaki_exp_kernel(const GroupEntry
 
 // Ozaki slices of every problem (A packed, B stacked): blocks [0, a_blocks) take
 // 8 rows of some A (warp per row, lanes over 4-column groups); the rest take
-// one 32 (k) x 32 (n) tile of some B, transposed.
+// one 32 (k) x 64 (n) tile of some B, transposed.
 template <int S>
 __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEntry* __restrict__ g, int count,
                                                                   int a_blocks) {
-  __shared__ double tile[32][33];
+  __shared__ double tile[32][65];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int b = blockIdx.x;
   if (b < a_blocks) {
@@ -195,9 +195,18 @@ __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEnt
     const int nc4 = (int)(e.kpad / 4);
     for (int gi = lane; gi < nc4; gi += 32) {
       const int c = gi * 4;
+      double v[4];
+      if (c + 4 <= e.k) {
+        const double2 v0 = *reinterpret_cast<const double2*>(src + c);  // 16-byte rows, c % 4 == 0
+        const double2 v1 = *reinterpret_cast<const double2*>(src + c + 2);
+        v[0] = v0.x, v[1] = v0.y, v[2] = v1.x, v[3] = v1.y;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = c + j < e.k ? src[c + j] : 0.0;
+      }
       int8_t q[4][S];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) slice_value<S>(c + j < e.k ? src[c + j] : 0.0, ex, q[j]);
+      for (int j = 0; j < 4; ++j) slice_value<S>(v[j], ex, q[j]);
 #pragma unroll
       for (int t = 0; t < S; ++t) {
         const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
@@ -207,25 +216,49 @@ __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEnt
     }
     return;
   }
+  // one 32 (k) x 64 (n) tile of some B: 16 lanes load 64 doubles of a row; a
+  // lane slices 4 consecutive k of one column (one 4-byte store per slice)
   b -= a_blocks;
   const GroupEntry& e = g[find_entry<1>(g, count, b)];
   const int t = b - e.pre_b_start;
-  const int tiles_n32 = (e.n + 31) / 32;
-  const int k0 = (t / tiles_n32) * 32, n0 = (t % tiles_n32) * 32;
+  const int tiles_n64 = (e.n + 63) / 64;
+  const int k0 = (t / tiles_n64) * 32, n0 = (t % tiles_n64) * 64;
   const double* B = static_cast<const double*>(e.B);
-  for (int i = warp; i < 32; i += 8) {
-    const int k = k0 + i, n = n0 + lane;
-    tile[i][lane] = (k < e.k && n < e.n) ? B[(int64_t)k * e.ldb + n] : 0.0;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const int i = p * 16 + tid / 16, c = (tid % 16) * 4;
+    const int k = k0 + i, n = n0 + c;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (k < e.k) {
+      const double* src = B + (int64_t)k * e.ldb + n;
+      if (n + 4 <= e.n) {
+        const double2 v0 = *reinterpret_cast<const double2*>(src);
+        const double2 v1 = *reinterpret_cast<const double2*>(src + 2);
+        v[0] = v0.x, v[1] = v0.y, v[2] = v1.x, v[3] = v1.y;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = n + j < e.n ? src[j] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) tile[i][c + j] = v[j];
   }
   __syncthreads();
   int8_t* out = static_cast<int8_t*>(e.planes_b);
-  for (int i = warp; i < 32; i += 8) {
-    const int n = n0 + i, k = k0 + lane;
-    if (n < e.n && k < e.kpad) {
-      int8_t q[S];
-      slice_value<S>(tile[lane][i], e.eb[n], q);
 #pragma unroll
-      for (int s = 0; s < S; ++s) out[stacked_index<S>(n, k, e.n, s)] = q[s];
+  for (int p = 0; p < 2; ++p) {
+    const int item = p * 256 + tid, nl = item / 8, kq = item % 8;
+    const int n = n0 + nl, k = k0 + kq * 4;
+    if (n >= e.n) continue;
+    const int ex = e.eb[n];
+    int8_t q[4][S];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) slice_value<S>(tile[kq * 4 + j][nl], ex, q[j]);
+#pragma unroll
+    for (int s_ = 0; s_ < S; ++s_) {
+      const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
+                          ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
+      *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, e.n, s_)) = pk;
     }
   }
 }
@@ -305,7 +338,7 @@ cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr
     e.pre_a_start = pa;
     pa += (int)ceil_div(q.m, 8);
     e.pre_b_start = pb;
-    pb += L.kind == 2 ? (int)(ceil_div(e.kpad, 32) * ceil_div(q.n, 32)) : (int)(ceil_div(e.kpad, 64) * ceil_div(q.n, 64));
+    pb += L.kind == 2 ? (int)(ceil_div(e.kpad, 32) * ceil_div(q.n, 64)) : (int)(ceil_div(e.kpad, 64) * ceil_div(q.n, 64));
     e.exp_a_start = xa;
     xa += (int)ceil_div(q.m, 8);
     e.exp_b_start = xb;
