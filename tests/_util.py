@@ -68,3 +68,18 @@ def check_against_oracle(out, A, B, Cin, alpha, beta, epilogue, dtype, factor=1.
         raise AssertionError("%d of %d entries outside the bound; first at %s: out=%r ref=%r err=%.3e bound=%.3e"
                              % (bad.sum(), bad.size, tuple(i), out[tuple(i)], ref[tuple(i)], err[tuple(i)], b[tuple(i)]))
     return oracle.errors(out, ref)
+
+
+def bf16_bound(A, B, Cin, alpha, beta, nterms):
+    """|err| <= (c_split + 6 (k+2) u32) |alpha| (|A||B|) + 2 u32 |beta C| + 2 u32 |result|,
+    c_split = 3.1 * 2^-16 for BF16x3 (dropped lo*lo and the two residuals),
+    6 * 2^-24 for BF16x6."""
+    k = A.shape[1]
+    u = 2.0 ** -24
+    c_split = 3.1 * 2.0 ** -16 if nterms == 2 else 6.0 * u
+    absab = oracle.gemm(np.abs(A), np.abs(B))
+    ref = oracle.gemm(A, B, Cin, alpha, beta)
+    b = (c_split + 6 * (k + 2) * u) * abs(alpha) * absab + 2 * u * np.abs(ref) + 1e-30
+    if beta:
+        b += 2 * u * abs(beta) * np.abs(Cin.astype(np.float64))
+    return ref, b

@@ -11,7 +11,7 @@ import pytest
 
 import cucosma_b200 as cc
 import oracle
-from tests._util import expspread, to_dev, uniform
+from tests._util import bf16_bound, expspread, to_dev, uniform
 
 pytestmark = pytest.mark.gpu
 
@@ -40,21 +40,6 @@ def run(A, B, Cin, alpha, beta, precision, epilogue="none", slices=0, split_k=0,
     if keep_ws:
         return out, plan, (ws.cpu().numpy() if ws is not None else None)
     return out, plan
-
-
-def bf16_bound(A, B, Cin, alpha, beta, nterms):
-    """|err| <= (c_split + 6 (k+2) u32) |alpha| (|A||B|) + 2 u32 |beta C| + 2 u32 |result|,
-    c_split = 3.1 * 2^-16 for BF16x3 (dropped lo*lo and the two residuals),
-    6 * 2^-24 for BF16x6."""
-    k = A.shape[1]
-    u = 2.0 ** -24
-    c_split = 3.1 * 2.0 ** -16 if nterms == 2 else 6.0 * u
-    absab = oracle.gemm(np.abs(A), np.abs(B))
-    ref = oracle.gemm(A, B, Cin, alpha, beta)
-    b = (c_split + 6 * (k + 2) * u) * abs(alpha) * absab + 2 * u * np.abs(ref) + 1e-30
-    if beta:
-        b += 2 * u * abs(beta) * np.abs(Cin.astype(np.float64))
-    return ref, b
 
 
 SHAPES = [(1, 1, 1), (7, 5, 3), (128, 256, 32), (129, 257, 33), (300, 200, 100), (256, 512, 1024), (1000, 64, 77),
