@@ -75,8 +75,8 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
   }
   pl.splits = (int)ceil_div(pl.kblocks, pl.kb_per_split);
   // Raster band (tiles of M visited together): measured best at 8192^3 and
-  // 16384^3 -- 16 for the BF16 paths (128 x 256 tiles), 8 for Ozaki.
-  pl.band = d->swizzle > 0 ? d->swizzle : (pl.kind == 2 ? 8 : 16);
+  // 16384^3 -- 16 for the BF16 paths (128 x 256 tiles), 4 for Ozaki.
+  pl.band = d->swizzle > 0 ? d->swizzle : (pl.kind == 2 ? 4 : 16);
   const int es_in = pl.kind == 2 ? 1 : 2;
   const int es_out = pl.kind == 2 ? 8 : 4;
   size_t off = 0;

@@ -591,8 +591,9 @@ struct TraitsBase {
 };
 
 // K-blocks (32 wide) the tensor cores accumulate before the epilogue adds
-// the chunk into its FP32 registers.
-constexpr int kPromoteChunk = 4;
+// the chunk into its FP32 registers (8: measured 4.7 % faster than 4 on
+// BF16x3 at 8192^3 for a 1.6 % larger normwise error).
+constexpr int kPromoteChunk = 8;
 
 // BF16x3: (lo,hi), (hi,lo), (hi,hi) -- small terms first -- one accumulator.
 // Term tables: for term t, the A plane a[t], the B plane b[t], the
