@@ -194,6 +194,33 @@ def gemm(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none", spl
     return Cm
 
 
+def host_desc(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none", split_k=0, slices=0, tile=0):
+    """Descriptor for cucosma_gemm_host from host (CPU) tensors: ld* are their row strides."""
+    return make_desc(A, B, Cm, alpha, beta, precision, epilogue, split_k, 0, slices, tile)
+
+
+def host_buffer(desc, device=None):
+    """Device buffer of cucosma_gemm_host_buffer_size bytes (256-byte aligned)."""
+    import torch
+
+    n = C.c_size_t(0)
+    check(lib().cucosma_gemm_host_buffer_size(C.byref(desc), C.byref(n)), "cucosma_gemm_host_buffer_size")
+    return torch.empty(n.value, dtype=torch.uint8, device=device or "cuda")
+
+
+def gemm_host(A, B, Cm, alpha=1.0, beta=0.0, precision="native", epilogue="none", split_k=0, slices=0, tile=0,
+              buffer=None, stream=None):
+    """C <- epi(alpha*A@B + beta*C) on host (CPU, ideally pinned) tensors through
+    cucosma_gemm_host: the copies in and out overlap the row-block GEMMs.
+    Asynchronous on the stream; synchronise before reading C."""
+    d = host_desc(A, B, Cm, alpha, beta, precision, epilogue, split_k, slices, tile)
+    if buffer is None:
+        buffer = host_buffer(d)
+    check(lib().cucosma_gemm_host(C.byref(d), A.data_ptr(), B.data_ptr(), Cm.data_ptr(), buffer.data_ptr(),
+                                  buffer.numel(), _stream_handle(stream)), "cucosma_gemm_host")
+    return Cm
+
+
 def cosma_sgemm(A, B, Cm, alpha=1.0, beta=0.0, stream=None):
     """The reference-shaped entry point: cosmaSgemm(A, lda, B, ldb, C, ldc) with
     M, N, K from the tensor shapes (FP32 -> cucosma_sgemm, FP64 -> cucosma_dgemm)."""

@@ -38,6 +38,8 @@ def bind(L):
         "cucosma_tune_cache_load": ([C.c_char_p], C.c_int),
         "cucosma_tune_cache_clear": ([], C.c_int),
         "cucosma_tune_cache_size": ([], C.c_int),
+        "cucosma_gemm_host_buffer_size": ([C.POINTER(GemmDesc), C.POINTER(sz)], C.c_int),
+        "cucosma_gemm_host": ([C.POINTER(GemmDesc), vp, vp, vp, vp, sz, vp], C.c_int),
         "cucosma_gemm_backward_workspace_size": ([C.POINTER(GemmDesc), C.POINTER(sz)], C.c_int),
         "cucosma_gemm_backward": ([C.POINTER(GemmDesc), vp, vp, vp, C.c_int64, vp, C.c_int64, vp, C.c_int64, vp,
                                    C.c_int64, vp, sz, vp], C.c_int),

@@ -1,0 +1,175 @@
+// host.cu -- GEMM on host (pinned) buffers with the copies overlapped.
+//
+// No counterpart in the reference, whose callers copy operands in and out
+// themselves around cosmaSgemm (test_correctness.h).  The caller's device
+// buffer holds device copies of A, B and C and the GEMM workspace.  B goes
+// over first; A (and C when beta != 0) follow in row blocks, each block's
+// GEMM (a row slice of the problem through the regular entry point) runs as
+// soon as its rows have arrived, and its C rows go back while later blocks
+// still copy in -- so the host-to-device and device-to-host transfers run
+// concurrently with each other and with the compute.  Three streams per
+// device (created on first use) carry the copies in, the GEMMs and the copies
+// out; the caller's stream waits for the last copy out.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/cucosma.h"
+#include "api_internal.cuh"
+#include "common.cuh"
+
+namespace cucosma {
+namespace {
+
+constexpr int kMaxBlocks = 16;
+
+struct HostStreams {
+  cudaStream_t in = nullptr, gemm = nullptr, out = nullptr;
+  cudaEvent_t start = nullptr, b_in = nullptr, done = nullptr;
+  cudaEvent_t a_in[kMaxBlocks] = {}, c_ready[kMaxBlocks] = {};
+  bool ok = false;
+};
+
+HostStreams* streams_for_current_device() {
+  static std::mutex mu;
+  static HostStreams per_device[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  HostStreams& h = per_device[dev];
+  if (!h.ok) {
+    bool good = cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&h.gemm, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&h.b_in, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; good && i < kMaxBlocks; ++i)
+      good = cudaEventCreateWithFlags(&h.a_in[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&h.c_ready[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!good) return nullptr;
+    h.ok = true;
+  }
+  return &h;
+}
+
+size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct HostLayout {
+  int blocks;
+  int64_t rows_per_block;
+  size_t off_a, off_b, off_c, off_ws, ws_bytes, total;
+  int64_t lda, ldb, ldc;  // device row strides (16-byte rows)
+};
+
+cucosma_status host_layout(const cucosma_gemm_desc* d, HostLayout* L) {
+  if (!d || d->m <= 0 || d->n <= 0 || d->k <= 0) return CUCOSMA_STATUS_INVALID_VALUE;
+  const int es = d->dtype == CUCOSMA_R_32F ? 4 : 8;
+  const int64_t vec = 16 / es;
+  L->lda = round_up(d->k, vec);
+  L->ldb = round_up(d->n, vec);
+  L->ldc = round_up(d->n, vec);
+  // Row blocks of at least 256 rows, at most kMaxBlocks of them.
+  L->blocks = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxBlocks / 2, d->m / 256));
+  L->rows_per_block = round_up(ceil_div(d->m, L->blocks), 128);
+  L->blocks = (int)ceil_div(d->m, L->rows_per_block);
+  // The regular entry point's workspace for a full row block and for the
+  // last (possibly shorter) one; the larger serves every block in turn.
+  L->ws_bytes = 0;
+  const int64_t sizes[2] = {std::min<int64_t>(d->m, L->rows_per_block),
+                            d->m - (int64_t)(L->blocks - 1) * L->rows_per_block};
+  for (int64_t rows : sizes) {
+    cucosma_gemm_desc sub = *d;
+    sub.m = rows;
+    sub.lda = L->lda;
+    sub.ldb = L->ldb;
+    sub.ldc = L->ldc;
+    size_t b = 0;
+    cucosma_status s = cucosma_gemm_workspace_size(&sub, &b);
+    if (s != CUCOSMA_STATUS_SUCCESS) return s;
+    L->ws_bytes = std::max(L->ws_bytes, b);
+  }
+  size_t off = 0;
+  L->off_a = off;
+  off = al256(off + (size_t)d->m * L->lda * es);
+  L->off_b = off;
+  off = al256(off + (size_t)d->k * L->ldb * es);
+  L->off_c = off;
+  off = al256(off + (size_t)d->m * L->ldc * es);
+  L->off_ws = off;
+  off = al256(off + L->ws_bytes);
+  L->total = off;
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
+}  // namespace
+}  // namespace cucosma
+
+using namespace cucosma;
+
+extern "C" cucosma_status cucosma_gemm_host_buffer_size(const cucosma_gemm_desc* d, size_t* bytes) {
+  if (!bytes) return CUCOSMA_STATUS_INVALID_VALUE;
+  HostLayout L;
+  cucosma_status s = host_layout(d, &L);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  *bytes = L.total;
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
+extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
+                                            void* device_buffer, size_t buffer_bytes, void* stream) {
+  HostLayout L;
+  cucosma_status s = host_layout(d, &L);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  if (!A || !B || !C) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (d->lda < d->k || d->ldb < d->n || d->ldc < d->n) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (!device_buffer || buffer_bytes < L.total) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
+  if (reinterpret_cast<uintptr_t>(device_buffer) & 255) return CUCOSMA_STATUS_MISALIGNED;
+  HostStreams* h = streams_for_current_device();
+  if (!h) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  const size_t es = d->dtype == CUCOSMA_R_32F ? 4 : 8;
+  uint8_t* w = static_cast<uint8_t*>(device_buffer);
+  uint8_t* dA = w + L.off_a;
+  uint8_t* dB = w + L.off_b;
+  uint8_t* dC = w + L.off_c;
+  void* ws = L.ws_bytes ? w + L.off_ws : nullptr;
+  const uint8_t* hA = static_cast<const uint8_t*>(A);
+  const uint8_t* hB = static_cast<const uint8_t*>(B);
+  uint8_t* hC = static_cast<uint8_t*>(C);
+  cudaStream_t caller = static_cast<cudaStream_t>(stream);
+  auto fail = [](cudaError_t e) { return e != cudaSuccess; };
+
+  // Everything starts after the work already queued on the caller's stream.
+  if (fail(cudaEventRecord(h->start, caller)) || fail(cudaStreamWaitEvent(h->in, h->start, 0)) ||
+      fail(cudaStreamWaitEvent(h->gemm, h->start, 0)) || fail(cudaStreamWaitEvent(h->out, h->start, 0)))
+    return CUCOSMA_STATUS_LAUNCH_FAILED;
+  if (fail(cudaMemcpy2DAsync(dB, L.ldb * es, hB, d->ldb * es, d->n * es, d->k, cudaMemcpyHostToDevice, h->in)) ||
+      fail(cudaEventRecord(h->b_in, h->in)) || fail(cudaStreamWaitEvent(h->gemm, h->b_in, 0)))
+    return CUCOSMA_STATUS_LAUNCH_FAILED;
+  for (int i = 0; i < L.blocks; ++i) {
+    const int64_t r0 = i * L.rows_per_block, rows = std::min<int64_t>(L.rows_per_block, d->m - r0);
+    if (fail(cudaMemcpy2DAsync(dA + r0 * L.lda * es, L.lda * es, hA + r0 * d->lda * es, d->lda * es, d->k * es, rows,
+                               cudaMemcpyHostToDevice, h->in)))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    if (d->beta != 0.0 &&
+        fail(cudaMemcpy2DAsync(dC + r0 * L.ldc * es, L.ldc * es, hC + r0 * d->ldc * es, d->ldc * es, d->n * es, rows,
+                               cudaMemcpyHostToDevice, h->in)))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    if (fail(cudaEventRecord(h->a_in[i], h->in)) || fail(cudaStreamWaitEvent(h->gemm, h->a_in[i], 0)))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    cucosma_gemm_desc sub = *d;
+    sub.m = rows;
+    sub.lda = L.lda;
+    sub.ldb = L.ldb;
+    sub.ldc = L.ldc;
+    s = cucosma_gemm(&sub, dA + r0 * L.lda * es, dB, dC + r0 * L.ldc * es, ws, L.ws_bytes, h->gemm);
+    if (s != CUCOSMA_STATUS_SUCCESS) return s;
+    if (fail(cudaEventRecord(h->c_ready[i], h->gemm)) || fail(cudaStreamWaitEvent(h->out, h->c_ready[i], 0)) ||
+        fail(cudaMemcpy2DAsync(hC + r0 * d->ldc * es, d->ldc * es, dC + r0 * L.ldc * es, L.ldc * es, d->n * es, rows,
+                               cudaMemcpyDeviceToHost, h->out)))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+  }
+  if (fail(cudaEventRecord(h->done, h->out)) || fail(cudaStreamWaitEvent(caller, h->done, 0)))
+    return CUCOSMA_STATUS_LAUNCH_FAILED;
+  return CUCOSMA_STATUS_SUCCESS;
+}

@@ -175,6 +175,21 @@ CUCOSMA_API cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* fwd, c
                                                  int64_t ldda, void* dB, int64_t lddb, void* workspace,
                                                  size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------ host buffers
+ * C = epi(alpha*A*B + beta*C) with A, B and C in host memory (pinned, for the
+ * copies to overlap; lda/ldb/ldc are the host row strides).  No counterpart
+ * in the reference, whose callers copy around cosmaSgemm themselves.  B is
+ * copied first; A (and C when beta != 0) follow in row blocks, each block's
+ * GEMM runs when its rows have arrived and its C rows are copied back while
+ * later blocks still copy in, on three library streams per device (created
+ * by the first call on that device) ordered after the work queued on stream;
+ * stream waits for the last copy back.  device_buffer (256-byte aligned, of
+ * cucosma_gemm_host_buffer_size bytes) holds the device copies and the GEMM
+ * workspace; calls sharing it must be ordered on the same stream. */
+CUCOSMA_API cucosma_status cucosma_gemm_host_buffer_size(const cucosma_gemm_desc* d, size_t* bytes);
+CUCOSMA_API cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
+                                             void* device_buffer, size_t buffer_bytes, void* stream);
+
 /* ---------------------------------------------------------------- grouped
  * Many independent GEMMs of uneven sizes in one persistent launch (no
  * counterpart in the reference, whose sizes are compile-time macros: one
