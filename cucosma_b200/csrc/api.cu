@@ -152,14 +152,26 @@ NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws) {
   if (splits <= 0) {
     splits = 1;
     // Resident CTA slots: two per SM for FP32 (128 registers), one for FP64.
+    // Model: a CTA takes about 2.1 us per 16-deep k-block either way (half an
+    // SM's FP32 rate, or a whole SM's FP64 rate), so the GEMM takes
+    // ceil(tiles * s / slots) waves of ceil(kblocks / s) k-blocks; s > 1 adds
+    // a reduction that reads and writes s partial planes at HBM speed.  The
+    // s with the smallest modelled time wins (>= 8 k-blocks per split, within
+    // max_ws); this fills partial waves that a single split leaves idle.
     const int64_t slots = (int64_t)sms * (fp32 ? simt::Cfg<float>::CTAS_PER_SM : simt::Cfg<double>::CTAS_PER_SM);
-    if (tiles < slots) {
-      // Fill one wave of slots (rounding down, so no partial second wave)
-      // while keeping >= 8 k-blocks per split; within max_ws.
-      splits = std::max<int64_t>(1, std::min<int64_t>(slots / tiles, kblocks / 8));
-      const size_t per_split = (size_t)d->m * (size_t)round_up(d->n, vec) * es;
-      if (splits > 1 && per_split > 0 && (size_t)splits * per_split > max_ws)
-        splits = std::max<int64_t>(1, (int64_t)(max_ws / per_split));
+    const double kblock_us = 2.1;
+    const size_t per_split = (size_t)d->m * (size_t)round_up(d->n, vec) * es;
+    const int64_t smax = std::max<int64_t>(1, std::min<int64_t>(kblocks / 8, 512));
+    double best = 1e300;
+    for (int64_t s = 1; s <= smax; ++s) {
+      if (s > 1 && (size_t)s * per_split > max_ws) break;
+      const double waves = (double)ceil_div(tiles * s, slots);
+      double t = waves * (double)ceil_div(kblocks, s) * kblock_us;
+      if (s > 1) t += 4.0 + 2.0 * (double)s * (double)per_split / 6.0e6;  // us: launch + s planes in and out
+      if (t < best * 0.98) {  // a clear gain, so ties keep the smaller split
+        best = t;
+        splits = s;
+      }
     }
   }
   splits = std::max<int64_t>(1, std::min<int64_t>(splits, kblocks));

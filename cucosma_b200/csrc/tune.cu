@@ -131,6 +131,11 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
   std::vector<int> tiles = {0};
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
     bands = {1, 2, 4, 8};
+    // a skinny shape: its kernel (tile 0, no block remap) against the tile kernel (tile 1)
+    if (pi.tile_m != simt::BM) {
+      bands = {1};
+      tiles = {0, 1};
+    }
   } else {
     bands = {8, 4, 16};
     if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = {0, 1, 2};

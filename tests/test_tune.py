@@ -44,7 +44,9 @@ def test_tune_then_use(cuda, tmp_path, precision, dtype):
     assert cc.tune_cache_size() == 1
     dC = to_dev(Cin)
     plan = cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))
-    assert plan["splits"] == r["split_k"] or r["split_k"] > plan["splits"] == (-(-k // plan["tile_k"]))
+    # a forced split count s becomes ceil(k / kchunk) splits, kchunk = round_up(ceil(k / s), tile_k)
+    kchunk = -(-(-(-k // r["split_k"])) // plan["tile_k"]) * plan["tile_k"]
+    assert plan["splits"] == min(r["split_k"], -(-k // kchunk))
     cc.gemm(dA, dB, dC, 1.0, 0.5, precision=precision)
     torch.cuda.synchronize()
     out = dC.cpu().numpy()
@@ -67,3 +69,26 @@ def test_tune_then_use(cuda, tmp_path, precision, dtype):
     assert p_on["splits"] == plan["splits"]
     cc.tune_cache_clear()
     assert p_off["splits"] == cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))["splits"]
+
+
+@pytest.mark.gpu
+def test_tune_skinny_shape_compares_kernels(cuda):
+    """A thin shape: the tuner weighs the skinny kernel (tile 0) against the
+    128 x 128 tile kernel (tile 1) and later calls use its pick correctly."""
+    import torch
+
+    cc.tune_cache_clear()
+    m, n, k = 4, 8, 200000
+    A, B = uniform(11, (m, k)), uniform(12, (k, n))
+    dA, dB = to_dev(A), to_dev(B)
+    scratch = to_dev(np.zeros((m, n), np.float32))
+    ws = torch.empty(64 << 20, dtype=torch.uint8, device="cuda")
+    r = cc.tune(dA, dB, scratch, 1.0, 0.0, workspace=ws)
+    print(r)
+    assert r["candidates"] >= 2 and r["tile"] in (0, 1)
+    dC = to_dev(np.zeros((m, n), np.float32))
+    cc.gemm(dA, dB, dC, 1.0, 0.0, workspace=ws)
+    torch.cuda.synchronize()
+    check_against_oracle(dC.cpu().numpy(), A, B, np.zeros((m, n), np.float32), 1.0, 0.0, oracle.EPI_NONE,
+                         np.float32)
+    cc.tune_cache_clear()
