@@ -217,7 +217,15 @@ __global__ void __launch_bounds__(256)
   const int64_t r = o / n, c = o - r * n;
   const T* w = ws + r * ldw + c;
   T s = T(0);
-  for (int z = lane; z < splits; z += 32) s += w[(int64_t)z * split_stride];
+  int z = lane;
+  for (; z + 32 * 7 < splits; z += 32 * 8) {  // loads of a batch issued before its adds (order kept)
+    T v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = w[(int64_t)(z + 32 * j) * split_stride];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += v[j];
+  }
+  for (; z < splits; z += 32) s += w[(int64_t)z * split_stride];
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   if (lane == 0) {
