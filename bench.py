@@ -22,7 +22,7 @@ on all host threads.
 Multi-GPU: the path does not shard (one GEMM per GPU); --gpus N runs N
 independent replicas, one per rank, and reports the aggregate.
 
---precision-sweep (not part of the driver contract) prints one JSON line per
+--precision-sweep (a separate mode beside the one-line benchmark) prints one JSON line per
 (size, value distribution, path): sizes 8192 and 16384, entries uniform[-1, 1]
 or sign * exp(N(0, sigma = 8)), paths native FP32, BF16x3, BF16x6, native FP64
 and Ozaki with 6..9 slices; TFLOP/s and the max / mean relative and normwise
