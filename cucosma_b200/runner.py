@@ -125,6 +125,9 @@ def run_row(row, args, flush, gen_seed):
     es = 8 if dtype == torch.float64 else 4
     if (m * k + k * n + m * n) * es > args.max_gb * 1e9:
         return None, None, "skipped: operands exceed --max-gb"
+    if (args.precision == "ozaki") != (dtype == torch.float64) and args.precision != "native":
+        return None, None, "skipped: %s needs %s rows" % (args.precision, "double" if args.precision == "ozaki"
+                                                            else "float")
     g = torch.Generator(device="cuda")
     g.manual_seed(gen_seed)
     A, B = pitched(m, k, dtype, g), pitched(k, n, dtype, g)
