@@ -138,42 +138,89 @@ cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B
 // --------------------------------------------------------------- planning
 static int simt_bk(int dtype) { return dtype == CUCOSMA_R_32F ? simt::Cfg<float>::BK : simt::Cfg<double>::BK; }
 
+// Modelled time (us) of the tile kernel with bm-row CTA tiles, `tiles` output
+// tiles and `s` K splits of `kblocks` 16-deep k-blocks in all, plus the
+// split-K reduction (s partial planes of per_split bytes in and out at HBM
+// speed, and a launch).  Fitted to B200 measurements of both FP32 tile
+// heights over square, flat, large-N and large-K shapes:
+//   * a 128 x 128 x 16 k-block step takes kUnitUs of an SM holding 16 warps
+//     (FP64: kUnitUsF64 a CTA, one CTA an SM);
+//   * an SM holding fewer warps runs at occupancy_rate() of that (one 4-warp
+//     CTA alone: 0.71; 8 warps: 0.91);
+//   * the 64-row CTAs do a 64-row step in 0.95 of half a 128-row step (four
+//     4-warp CTAs an SM stall less at the per-stage barrier than two 8-warp
+//     ones);
+//   * whole waves of resident CTAs run at full occupancy, and the last,
+//     partial wave at the occupancy it leaves.
+namespace {
+constexpr double kUnitUs = 1.45, kUnitUsF64 = 2.4, kTile64Factor = 0.95;
+double occupancy_rate(int warps) {
+  return warps >= 16 ? 1.0 : warps >= 14 ? 0.99 : warps >= 12 ? 0.97 : warps >= 10 ? 0.95 : warps >= 8 ? 0.91
+                       : warps >= 6 ? 0.8 : 0.71;
+}
+double native_time_us(int bm, bool fp32, int64_t tiles, int64_t s, int64_t kblocks, int sms, size_t per_split) {
+  const int per_sm = fp32 ? (bm == 64 ? simt::SgemmShape<64>::kCtasPerSm : simt::SgemmShape<128>::kCtasPerSm)
+                          : simt::Cfg<double>::CTAS_PER_SM;
+  const int warps_per_cta = fp32 ? bm / 16 : 16;  // FP64: one CTA fills its SM's FP64 rate
+  const double step = fp32 ? kUnitUs * (bm == 64 ? 0.5 * kTile64Factor : 1.0) : kUnitUsF64;  // one CTA k-block, full SM
+  const int64_t ctas = tiles * s, slots = (int64_t)sms * per_sm;
+  const double kbs = (double)ceil_div(kblocks, s);
+  const int64_t waves = ctas / slots, rest = ctas - waves * slots;
+  double t = (double)waves * kbs * per_sm * step;
+  if (rest > 0) {
+    const int r = (int)ceil_div(rest, (int64_t)sms);  // CTAs on the busiest SM of the last wave
+    t += kbs * r * step / occupancy_rate(r * warps_per_cta);
+  }
+  if (s > 1) t += 2.0 + 2.0 * (double)s * (double)per_split / 6.0e6;
+  return t;
+}
+}  // namespace
+
 NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws) {
   NativePlan p{};
   const bool fp32 = d->dtype == CUCOSMA_R_32F;
   const int bk = simt_bk(d->dtype);
   const int es = fp32 ? 4 : 8;
   const int vec = 16 / es;
-  p.tiles_m = (int)ceil_div(d->m, simt::BM);
-  p.tiles_n = (int)ceil_div(d->n, simt::BN);
-  const int64_t tiles = (int64_t)p.tiles_m * p.tiles_n;
   const int64_t kblocks = std::max<int64_t>(1, ceil_div(d->k, bk));
+  const size_t per_split = (size_t)d->m * (size_t)round_up(d->n, vec) * es;
+  // Tile heights to consider: tile id 1 = 128 rows, 2 = 64 rows (FP32), 0 = both.
+  int heights[2] = {simt::BM, 64};
+  int nh = 1;
+  if (fp32 && d->tile == 2) heights[0] = 64;
+  else if (fp32 && d->tile == 0) nh = 2;
+  const int64_t tiles_n = ceil_div(d->n, simt::BN);
   int64_t splits = d->split_k;
+  int bm = heights[0];
   if (splits <= 0) {
-    splits = 1;
-    // Resident CTA slots: two per SM for FP32 (128 registers), one for FP64.
-    // Model: a CTA takes about 2.1 us per 16-deep k-block either way (half an
-    // SM's FP32 rate, or a whole SM's FP64 rate), so the GEMM takes
-    // ceil(tiles * s / slots) waves of ceil(kblocks / s) k-blocks; s > 1 adds
-    // a reduction that reads and writes s partial planes at HBM speed.  The
-    // s with the smallest modelled time wins (>= 8 k-blocks per split, within
-    // max_ws); this fills partial waves that a single split leaves idle.
-    const int64_t slots = (int64_t)sms * (fp32 ? simt::Cfg<float>::CTAS_PER_SM : simt::Cfg<double>::CTAS_PER_SM);
-    const double kblock_us = 2.1;
-    const size_t per_split = (size_t)d->m * (size_t)round_up(d->n, vec) * es;
-    const int64_t smax = std::max<int64_t>(1, std::min<int64_t>(kblocks / 8, 512));
+    // The (height, split) pair with the smallest modelled time wins; splits
+    // keep >= 4 k-blocks each and fit max_ws, and a candidate must beat the
+    // best so far by 2 % (ties keep the taller tile and the smaller split).
+    const int64_t smax = std::max<int64_t>(1, std::min<int64_t>(kblocks / 4, 512));
     double best = 1e300;
-    for (int64_t s = 1; s <= smax; ++s) {
-      if (s > 1 && (size_t)s * per_split > max_ws) break;
-      const double waves = (double)ceil_div(tiles * s, slots);
-      double t = waves * (double)ceil_div(kblocks, s) * kblock_us;
-      if (s > 1) t += 4.0 + 2.0 * (double)s * (double)per_split / 6.0e6;  // us: launch + s planes in and out
-      if (t < best * 0.98) {  // a clear gain, so ties keep the smaller split
-        best = t;
-        splits = s;
+    splits = 1;
+    for (int h = 0; h < nh; ++h) {
+      const int64_t tiles = ceil_div(d->m, heights[h]) * tiles_n;
+      for (int64_t s = 1; s <= smax; ++s) {
+        if (s > 1 && (size_t)s * per_split > max_ws) break;
+        const double t = native_time_us(heights[h], fp32, tiles, s, kblocks, sms, per_split);
+        if (t < best * 0.98) {
+          best = t;
+          splits = s;
+          bm = heights[h];
+        }
       }
     }
+  } else if (nh == 2) {
+    // forced split: the height with the smaller modelled time
+    const int64_t s = std::min<int64_t>(splits, kblocks);
+    const double t128 = native_time_us(128, fp32, ceil_div(d->m, 128) * tiles_n, s, kblocks, sms, per_split);
+    const double t64 = native_time_us(64, fp32, ceil_div(d->m, 64) * tiles_n, s, kblocks, sms, per_split);
+    bm = t64 < t128 * 0.98 ? 64 : 128;
   }
+  p.bm = bm;
+  p.tiles_m = (int)ceil_div(d->m, bm);
+  p.tiles_n = (int)tiles_n;
   splits = std::max<int64_t>(1, std::min<int64_t>(splits, kblocks));
   splits = std::min<int64_t>(splits, 65535);
   int64_t kchunk = round_up(ceil_div(std::max<int64_t>(d->k, 1), splits), bk);
@@ -194,7 +241,7 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
   constexpr int BK = simt::Cfg<T>::BK;
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   CUtensorMap tmA, tmB;
-  if (!encode_2d(&tmA, dt, sizeof(T), A, d->k, d->m, d->lda, BK, simt::BM, simt::Cfg<T>::A_SWIZZLE))
+  if (!encode_2d(&tmA, dt, sizeof(T), A, d->k, d->m, d->lda, BK, pl.bm, simt::Cfg<T>::A_SWIZZLE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (!encode_2d(&tmB, dt, sizeof(T), B, d->n, d->k, d->ldb, simt::BN, BK, CU_TENSOR_MAP_SWIZZLE_NONE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
@@ -222,7 +269,7 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
     p.ldo = d->ldc;
   }
   prof_begin(st);
-  if (simt::launch_gemm<T>(tmA, tmB, p, st) != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  if (simt::launch_gemm<T>(tmA, tmB, p, pl.bm, st) != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
   prof_end(st);
   note_launches(pl.splits > 1 ? 2 : 1);
   if (pl.splits > 1) {
@@ -404,7 +451,7 @@ extern "C" cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cuco
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
     const NativePlan pl = plan_native(d, di->sms);
     info->path = 0;
-    info->tile_m = simt::BM;
+    info->tile_m = pl.bm;
     info->tile_n = simt::BN;
     info->tile_k = simt_bk(d->dtype);
     info->splits = pl.splits;

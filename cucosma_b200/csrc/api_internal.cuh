@@ -20,12 +20,13 @@ struct WaitCtl;
 void wait_ctl(const DeviceInfo* di, int** status, unsigned long long* timeout_ns);
 
 struct NativePlan {
+  int bm;  // CTA tile rows: 128, or 64 (FP32 only); 128 columns either way
   int tiles_m, tiles_n, splits, swizzle;
   int64_t kchunk, ldw;
   size_t ws_bytes;
 };
-// Plan of the 128 x 128 tile kernel; an automatic split-K factor is chosen
-// so that its partial sums fit max_ws bytes.
+// Plan of the tile kernel (tile height and split-K factor); an automatic
+// split-K factor is chosen so that its partial sums fit max_ws bytes.
 NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws = SIZE_MAX);
 
 cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B, const void* C);

@@ -74,21 +74,23 @@ __device__ __forceinline__ void simt_store(const T (&acc)[8][8], const SimtParam
   }
 }
 
-// FP32 kernel.  A TMA ring of 4 stages; every A stage is transposed once in shared memory into a k-major buffer (double buffered),
-// so each k costs 2 LDS.128 for the 8 A values and 2 for the 8 B values of a
-// thread's 8x8 tile (thread rows are two groups of 4 consecutive rows).  The
-// one CTA barrier per stage that publishes the transposed tile also proves
-// that every warp finished the previous stage, so thread 0 refills that
-// stage right after it: no empty barriers, no producer wait on the critical
-// path.  128 registers: two CTAs per SM.
-namespace simt {
-constexpr int kLdT = BM + 4;  // k-major A row pitch (floats): 16-byte aligned rows
-}
-
-__global__ void __launch_bounds__(simt::kThreads, 2)
+// FP32 kernel, CTA tile BM_ x 128 with BM_ = 128 (8 warps, 4 stages, two
+// CTAs per SM) or 64 (4 warps, 3 stages, four CTAs per SM: twice the tiles
+// for shapes that leave SMs idle at 128 rows).  A TMA ring of stages; every A
+// stage is transposed once in shared memory into a k-major buffer (double
+// buffered), so each k costs 2 LDS.128 for the 8 A values and 2 for the 8 B
+// values of a thread's 8x8 tile (thread rows are two groups of 4 consecutive
+// rows).  The one CTA barrier per stage that publishes the transposed tile
+// also proves that every warp finished the previous stage, so thread 0
+// refills that stage right after it: no empty barriers, no producer wait on
+// the critical path.  128 registers a thread either way.
+template <int BM_>
+__global__ void __launch_bounds__(simt::SgemmShape<BM_>::kThreads, simt::SgemmShape<BM_>::kCtasPerSm)
     simt_sgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const SimtParams p) {
   using namespace simt;
+  using Shape = SgemmShape<BM_>;
+  constexpr int BM = BM_, STAGES = Shape::kStages, kLdT = Shape::kLdT;
   constexpr int BK = Cfg<float>::BK;  // 16
   constexpr int A_STAGE = BM * BK * 4, B_STAGE = BK * BN * 4;
   extern __shared__ uint8_t smem_raw[];
@@ -138,8 +140,8 @@ __global__ void __launch_bounds__(simt::kThreads, 2)
   const int tx = lane & 7, ty = lane >> 3;
   const int a_col = wm * 32 + ty * 4;  // this thread's rows: a_col + {0..3}, a_col + 16 + {0..3}
   const int b_col = wn * 64 + tx * 4;  // columns: b_col + {0..3}, b_col + 32 + {0..3}
-  // transpose role: thread handles row tr, k-half th (8 consecutive k)
-  const int tr = tid & (BM - 1), th = tid >> 7;
+  // transpose role (2*BM threads): thread handles row tr, k-half th (8 consecutive k)
+  const int tr = tid & (BM - 1), th = tid / BM;
   const int sw = (tr >> 1) & 3;  // 64-byte TMA swizzle of row tr: chunk ^ ((tr >> 1) & 3)
   const int c0 = ((2 * th) ^ sw) << 4, c1 = ((2 * th + 1) ^ sw) << 4;
   // acc[i][q]: row i, columns 2q and 2q + 1 of the thread's 8 (packed pairs
@@ -453,30 +455,41 @@ __global__ void scale_kernel(T* C, int64_t ldc, int m, int n, double beta_d, int
 namespace simt {
 
 template <typename T>
-size_t smem_bytes() {
+size_t smem_bytes(int bm) {
   constexpr int BK = Cfg<T>::BK;
-  // FP32 adds the double-buffered k-major copy of A (and needs no empty barriers)
-  constexpr size_t transposed = std::is_same<T, float>::value ? 2 * BK * kLdT * sizeof(float) : 0;
-  constexpr int stages = std::is_same<T, float>::value ? STAGES : kDStages;
-  return 1024 + stages * (BM * BK + BK * BN) * sizeof(T) + transposed + 2 * stages * sizeof(uint64_t);
+  if constexpr (std::is_same<T, float>::value) {
+    // stages of A and B, the double-buffered k-major copy of A, full barriers
+    const int stages = bm == 64 ? SgemmShape<64>::kStages : SgemmShape<128>::kStages;
+    return 1024 + (size_t)stages * (bm * BK + BK * BN) * sizeof(float) + 2 * BK * (bm + 4) * sizeof(float) +
+           2 * stages * sizeof(uint64_t);
+  } else {
+    return 1024 + kDStages * (BM * BK + BK * BN) * sizeof(T) + 2 * kDStages * sizeof(uint64_t);
+  }
 }
 
-// The GEMM kernel of each arithmetic type.
+// The GEMM kernel of each arithmetic type and CTA tile height.
 using GemmKernel = void (*)(const CUtensorMap, const CUtensorMap, const SimtParams);
 template <typename T>
-GemmKernel gemm_kernel() {
-  if constexpr (std::is_same<T, float>::value) return simt_sgemm_kernel;
+GemmKernel gemm_kernel(int bm) {
+  if constexpr (std::is_same<T, float>::value) return bm == 64 ? simt_sgemm_kernel<64> : simt_sgemm_kernel<128>;
   else return simt_dgemm_kernel;
+}
+template <typename T>
+int threads_of(int bm) {
+  return std::is_same<T, float>::value ? 2 * bm : kThreads;
 }
 
 template <typename T>
-cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, cudaStream_t stream) {
-  static bool attr_set = false;  // per process; the attribute is per function
-  const size_t smem = smem_bytes<T>();
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<T>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, int bm,
+                        cudaStream_t stream) {
+  if (!tile_rows_supported<T>(bm)) return cudaErrorInvalidValue;
+  static bool attr_set[2] = {false, false};  // per process and tile height; the attribute is per function
+  const size_t smem = smem_bytes<T>(bm);
+  bool& set = attr_set[bm == 64 ? 1 : 0];
+  if (!set) {
+    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<T>(bm), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    set = true;
   }
   dim3 grid;
   if (p.swizzle > 1) {
@@ -484,7 +497,7 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Si
   } else {
     grid = dim3(p.tiles_n, p.tiles_m, p.splits);
   }
-  gemm_kernel<T>()<<<grid, kThreads, smem, stream>>>(tmA, tmB, p);
+  gemm_kernel<T>(bm)<<<grid, threads_of<T>(bm), smem, stream>>>(tmA, tmB, p);
   return cudaGetLastError();
 }
 
@@ -511,27 +524,29 @@ cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, 
 }
 
 template <typename T>
-int occupancy() {
-  const size_t smem = smem_bytes<T>();
-  cudaFuncSetAttribute(gemm_kernel<T>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+int occupancy(int bm) {
+  if (!tile_rows_supported<T>(bm)) return 0;
+  const size_t smem = smem_bytes<T>(bm);
+  cudaFuncSetAttribute(gemm_kernel<T>(bm), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gemm_kernel<T>(), kThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gemm_kernel<T>(bm), threads_of<T>(bm), smem) !=
+      cudaSuccess)
     return 0;
   return blocks;
 }
-template int occupancy<float>();
-template int occupancy<double>();
+template int occupancy<float>(int);
+template int occupancy<double>(int);
 
-template cudaError_t launch_gemm<float>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
-template cudaError_t launch_gemm<double>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, cudaStream_t);
+template cudaError_t launch_gemm<float>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, int, cudaStream_t);
+template cudaError_t launch_gemm<double>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, int, cudaStream_t);
 template cudaError_t launch_reduce<float>(const float*, int64_t, int64_t, int, float*, int64_t, int, int, double, double,
                                           int, int, cudaStream_t);
 template cudaError_t launch_reduce<double>(const double*, int64_t, int64_t, int, double*, int64_t, int, int, double,
                                            double, int, int, cudaStream_t);
 template cudaError_t launch_scale<float>(float*, int64_t, int, int, double, int, int, cudaStream_t);
 template cudaError_t launch_scale<double>(double*, int64_t, int, int, double, int, int, cudaStream_t);
-template size_t smem_bytes<float>();
-template size_t smem_bytes<double>();
+template size_t smem_bytes<float>(int);
+template size_t smem_bytes<double>(int);
 
 }  // namespace simt
 }  // namespace cucosma

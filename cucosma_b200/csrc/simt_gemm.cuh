@@ -47,13 +47,31 @@ struct Cfg<double> {
   static constexpr CUtensorMapSwizzle A_SWIZZLE = CU_TENSOR_MAP_SWIZZLE_128B;
 };
 
+// CTA shapes of the FP32 kernel: BM_ x 128 tiles, 2 * BM_ threads, 128
+// registers a thread; BM_ = 128 or 64.  The 64-row shape keeps 16 warps an
+// SM (four CTAs) with three stages, so that four CTAs' shared memory fits.
+template <int BM_>
+struct SgemmShape {
+  static constexpr int kThreads = 2 * BM_;
+  static constexpr int kCtasPerSm = BM_ == 128 ? 2 : 4;
+  static constexpr int kStages = BM_ == 128 ? 4 : 3;
+  static constexpr int kLdT = BM_ + 4;  // k-major A row pitch (floats): 16-byte aligned rows
+};
+// CTA tile rows the native kernel of type T can run with (FP64: 128 only).
 template <typename T>
-size_t smem_bytes();
+inline bool tile_rows_supported(int bm) {
+  return bm == BM || (sizeof(T) == 4 && bm == 64);
+}
+
+// Dynamic shared memory of the GEMM kernel with bm-row CTA tiles.
+template <typename T>
+size_t smem_bytes(int bm = BM);
 // Resident CTAs per SM of the GEMM kernel (CUDA occupancy API).
 template <typename T>
-int occupancy();
+int occupancy(int bm = BM);
 template <typename T>
-cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, cudaStream_t stream);
+cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, int bm,
+                        cudaStream_t stream);
 template <typename T>
 cudaError_t launch_reduce(const T* ws, int64_t split_stride, int64_t ldw, int splits, T* C, int64_t ldc, int m, int n,
                           double alpha, double beta, int epi, int num_sms, cudaStream_t stream);

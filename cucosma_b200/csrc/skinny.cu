@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256)
 
 SkinnyPlan plan_skinny(int64_t m, int64_t n, int64_t k, int dtype_bytes, int split_k, int tile, int sms) {
   SkinnyPlan p{};
-  if (tile == 1 || m <= 0 || n <= 0 || k <= 0) return p;  // tile id 1: always the 128 x 128 tile kernel
+  if (tile == 1 || tile == 2 || m <= 0 || n <= 0 || k <= 0) return p;  // tile ids 1, 2: always the tile kernel
   const int vec = 16 / dtype_bytes;
   if (k <= skinny::kMaxSmallK) {
     p.kind = 1;

@@ -25,6 +25,7 @@
 #include "../../include/cucosma.h"
 #include "api_internal.cuh"
 #include "simt_gemm.cuh"
+#include "skinny.cuh"
 
 namespace cucosma {
 namespace {
@@ -131,8 +132,10 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
   std::vector<int> tiles = {0};
   if (d->precision == CUCOSMA_PRECISION_NATIVE) {
     bands = {1, 2, 4, 8};
+    // FP32 tile kernel: 128-row (tile 1) and 64-row (tile 2) CTA tiles
+    if (d->dtype == CUCOSMA_R_32F) tiles = {1, 2};
     // a skinny shape: its kernel (tile 0, no block remap) against the tile kernel (tile 1)
-    if (pi.tile_m != simt::BM) {
+    if (plan_skinny(d->m, d->n, d->k, d->dtype == CUCOSMA_R_32F ? 4 : 8, 0, 0, di->sms).kind) {
       bands = {1};
       tiles = {0, 1};
     }
@@ -203,7 +206,8 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
     cucosma_plan_info pk;
     cucosma_gemm_get_plan(&t, &pk);
     if (d->precision == CUCOSMA_PRECISION_NATIVE)
-      out->occupancy = d->dtype == CUCOSMA_R_32F ? simt::occupancy<float>() : simt::occupancy<double>();
+      out->occupancy = d->dtype == CUCOSMA_R_32F ? simt::occupancy<float>(pk.tile_m == 64 ? 64 : simt::BM)
+                                                 : simt::occupancy<double>();
     else
       out->occupancy = 1;  // persistent kernel, one CTA per SM by construction
     const int es = d->precision == CUCOSMA_PRECISION_NATIVE ? (d->dtype == CUCOSMA_R_32F ? 4 : 8)

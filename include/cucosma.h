@@ -78,7 +78,8 @@ typedef struct cucosma_gemm_desc {
   int32_t split_k;        /* SPLIT_K: 0 = library/tuner choice, >= 1 forced */
   int32_t swizzle;        /* SWIZZLE: 0 = library choice, >= 1 forced block-index remap width */
   int32_t tile;           /* 0 = library/tuner choice, else a kernel configuration id:
-                           * NATIVE 1 = always the 128 x 128 tile kernel (no skinny-shape kernels);
+                           * NATIVE 1 = always the 128 x 128 tile kernel (no skinny-shape kernels),
+                           *        2 = the 64 x 128 tile kernel (FP32; FP64 runs 128 x 128);
                            * BF16X3 1 = 128 x 256 without promotion, 2 = 128 x 128 promoted */
   int32_t flags;          /* 0, or CUCOSMA_FLAG_TEST_SKIP_STAGE */
 } cucosma_gemm_desc;

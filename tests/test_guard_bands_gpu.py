@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 SENTINEL = 1234.5
 
-CASES = [  # (precision, dtype, m, n, k, split_k)
+CASES = [  # (precision, dtype, m, n, k, split_k[, tile])
     ("native", np.float32, 130, 67, 45, 0), ("native", np.float32, 300, 200, 3000, 3),
     ("native", np.float64, 129, 257, 65, 0), ("native", np.float64, 77, 61, 900, 5),
     ("native", np.float32, 300, 1030, 3, 0), ("native", np.float32, 4, 9, 5000, 0),
@@ -23,14 +23,17 @@ CASES = [  # (precision, dtype, m, n, k, split_k)
     ("bf16x3", np.float32, 129, 257, 65, 0), ("bf16x3", np.float32, 200, 300, 3000, 2),
     ("bf16x6", np.float32, 130, 70, 45, 0), ("ozaki", np.float64, 129, 65, 33, 0),
     ("ozaki", np.float64, 70, 90, 3000, 3),
+    ("native", np.float32, 130, 67, 45, 0, 2), ("native", np.float32, 65, 300, 3000, 3, 2),
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=["%s_%s_%dx%dx%d_sk%d" % (c[0], np.dtype(c[1]).name, *c[2:]) for c in CASES])
+@pytest.mark.parametrize("case", CASES, ids=["%s_%s_%dx%dx%d_sk%d" % (c[0], np.dtype(c[1]).name, *c[2:6])
+                                             + ("_t%d" % c[6] if len(c) > 6 else "") for c in CASES])
 def test_writes_stay_inside_c(cuda, case):
     import torch
 
-    prec, dtype, m, n, k, split_k = case
+    prec, dtype, m, n, k, split_k = case[:6]
+    tile = case[6] if len(case) > 6 else 0
     es = np.dtype(dtype).itemsize
     A, B = uniform(1, (m, k), dtype), uniform(2, (k, n), dtype)
     dA, dB = to_dev(A), to_dev(B)
@@ -40,7 +43,7 @@ def test_writes_stay_inside_c(cuda, case):
     buf = torch.full((m + 4, ld), SENTINEL, dtype=tdt, device="cuda")
     C = buf[2:2 + m, :n]
     C.zero_()
-    cc.gemm(dA, dB, C, 1.0, 0.0, precision=prec, split_k=split_k)
+    cc.gemm(dA, dB, C, 1.0, 0.0, precision=prec, split_k=split_k, tile=tile)
     torch.cuda.synchronize()
     h = buf.cpu().numpy()
     region = np.zeros(h.shape, bool)

@@ -115,6 +115,47 @@ def test_deterministic_bitwise(cuda, dtype):
     assert all(np.array_equal(outs[0], o) for o in outs[1:])
 
 
+# The 64 x 128 CTA tile (tile id 2, FP32): partial tiles in both directions,
+# K below and above one stage, split-K, the fused epilogue and padded rows.
+TILE64 = [(1, 1, 1), (63, 129, 17), (64, 128, 16), (65, 300, 1000), (200, 70, 3), (513, 257, 700)]
+
+
+@pytest.mark.parametrize("split_k", [0, 3])
+@pytest.mark.parametrize("shape", TILE64, ids=["%dx%dx%d" % s for s in TILE64])
+def test_tile64_vs_oracle(cuda, shape, split_k):
+    m, n, k = shape
+    A, B, Cin = uniform(40, (m, k)), uniform(41, (k, n)), uniform(42, (m, n))
+    out = run(A, B, Cin, 1.25, 0.5, np.float32, tile=2, split_k=split_k)
+    check_against_oracle(out, A, B, Cin, 1.25, 0.5, oracle.EPI_NONE, np.float32)
+
+
+def test_tile64_sigmoid_padded(cuda):
+    A, B, Cin = uniform(43, (150, 301)), uniform(44, (301, 77)), uniform(45, (150, 77))
+    out = run(A, B, Cin, 1.0, 0.5, np.float32, epilogue="sigmoid", ld_pad=2, tile=2)
+    check_against_oracle(out, A, B, Cin, 1.0, 0.5, oracle.EPI_SIGMOID, np.float32)
+
+
+@pytest.mark.parametrize("split_k", [1, 4])
+def test_tile64_bitwise_equal_to_tile128(cuda, split_k):
+    """Both CTA heights accumulate every output over k in the same order
+    (ascending, one fmaf per k, splits added in order), so they agree bit for bit."""
+    A, B, Cin = uniform(46, (333, 2000)), uniform(47, (2000, 260)), uniform(48, (333, 260))
+    o128 = run(A, B, Cin, 1.0, 0.5, np.float32, tile=1, split_k=split_k)
+    o64 = run(A, B, Cin, 1.0, 0.5, np.float32, tile=2, split_k=split_k)
+    assert np.array_equal(o128, o64)
+
+
+def test_tile_ids_in_plan(cuda):
+    import torch
+
+    for dtype, want in ((torch.float32, 64), (torch.float64, 128)):
+        A = torch.zeros((300, 200), dtype=dtype, device="cuda")
+        B = torch.zeros((200, 500), dtype=dtype, device="cuda")
+        Cm = torch.zeros((300, 500), dtype=dtype, device="cuda")
+        assert cc.get_plan(cc.make_desc(A, B, Cm, tile=2))["tile_m"] == want
+        assert cc.get_plan(cc.make_desc(A, B, Cm, tile=1))["tile_m"] == 128
+
+
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "gemm_*.npz")))
 
 

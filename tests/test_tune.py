@@ -47,6 +47,11 @@ def test_tune_then_use(cuda, tmp_path, precision, dtype):
     # a forced split count s becomes ceil(k / kchunk) splits, kchunk = round_up(ceil(k / s), tile_k)
     kchunk = -(-(-(-k // r["split_k"])) // plan["tile_k"]) * plan["tile_k"]
     assert plan["splits"] == min(r["split_k"], -(-k // kchunk))
+    if precision == "native":
+        # the picked tile id fixes the CTA height: 1 -> 128 rows, 2 -> 64 (FP32)
+        assert r["tile"] in ((1, 2) if dtype == np.float32 else (0,))
+        if dtype == np.float32:
+            assert plan["tile_m"] == (64 if r["tile"] == 2 else 128)
     cc.gemm(dA, dB, dC, 1.0, 0.5, precision=precision)
     torch.cuda.synchronize()
     out = dC.cpu().numpy()
