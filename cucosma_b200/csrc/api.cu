@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -375,17 +376,19 @@ void prof_end(cudaStream_t st) {
 }
 
 // ------------------------------------------------- library-managed workspace
-void* managed_workspace(size_t bytes) {
+void* managed_workspace(size_t bytes, cudaStream_t st) {
+  // One buffer per (device, stream): calls queued on one stream run in order
+  // and can share it; calls on different streams may overlap on the GPU and
+  // must not.
   static std::mutex mu;
-  static std::vector<std::pair<void*, size_t>> per_dev;
+  static std::map<std::pair<int, cudaStream_t>, std::pair<void*, size_t>> slots;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   std::lock_guard<std::mutex> lk(mu);
-  if ((int)per_dev.size() <= dev) per_dev.resize(dev + 1, {nullptr, 0});
-  auto& slot = per_dev[dev];
+  auto& slot = slots[{dev, st}];
   if (slot.second < bytes) {
     if (slot.first) {
-      cudaDeviceSynchronize();  // the old buffer may still be in use by queued work
+      cudaStreamSynchronize(st);  // the old buffer may still be in use by queued work
       cudaFree(slot.first);
       slot = {nullptr, 0};
     }
@@ -493,7 +496,7 @@ static cucosma_status plain_gemm(int dtype, int m, int n, int k, T alpha, const 
   if (s != CUCOSMA_STATUS_SUCCESS) return s;
   void* ws = nullptr;
   if (need) {
-    ws = managed_workspace(need);
+    ws = managed_workspace(need, static_cast<cudaStream_t>(stream));
     if (!ws) return CUCOSMA_STATUS_ALLOC_FAILED;
   }
   return gemm(&d, A, B, C, ws, need, static_cast<cudaStream_t>(stream));

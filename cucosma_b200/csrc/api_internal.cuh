@@ -50,7 +50,7 @@ cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B,
 cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                           const DeviceInfo* di, cudaStream_t st, bool planes_ready);
 
-void* managed_workspace(size_t bytes);
+void* managed_workspace(size_t bytes, cudaStream_t st);
 
 // Tuning cache (tune.cu): when d leaves split_k, swizzle and tile at 0 and the
 // cache holds a choice for it, returns tmp filled with that choice, else d.

@@ -1,12 +1,28 @@
 // common.cuh -- shared device helpers: epilogue functors and the output
 // stage that applies C = epi(alpha*acc + beta*C).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "ptx.cuh"
 
 namespace cucosma {
+
+// Raises a kernel's dynamic shared memory limit to `bytes` once per device
+// (the attribute lives in each device's context, so a process that drives
+// several GPUs sets it on each); `done` is the kernel's mask of devices
+// already set.  Thread-safe: a race only repeats the idempotent call.
+inline cudaError_t ensure_smem_attr(const void* fn, int bytes, std::atomic<uint64_t>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev >= 0 && dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
 
 enum Epilogue : int { kEpiNone = 0, kEpiSigmoid = 1, kEpiRelu = 2 };
 

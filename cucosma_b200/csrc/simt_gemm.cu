@@ -483,14 +483,11 @@ template <typename T>
 cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const SimtParams& p, int bm,
                         cudaStream_t stream) {
   if (!tile_rows_supported<T>(bm)) return cudaErrorInvalidValue;
-  static bool attr_set[2] = {false, false};  // per process and tile height; the attribute is per function
+  static std::atomic<uint64_t> attr_set[2];  // devices done, per tile height (one kernel each)
   const size_t smem = smem_bytes<T>(bm);
-  bool& set = attr_set[bm == 64 ? 1 : 0];
-  if (!set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<T>(bm), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    set = true;
-  }
+  cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(gemm_kernel<T>(bm)), (int)smem,
+                                   attr_set[bm == 64 ? 1 : 0]);
+  if (e != cudaSuccess) return e;
   dim3 grid;
   if (p.swizzle > 1) {
     grid = dim3(p.tiles_n * p.swizzle, (unsigned)ceil_div(p.tiles_m, p.swizzle), p.splits);

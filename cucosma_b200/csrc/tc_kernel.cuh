@@ -666,12 +666,9 @@ struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, 
 
 template <class Tr>
 static cudaError_t launch(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p, int grid, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tr::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // devices whose context has the limit raised
+  cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(tc_gemm_kernel<Tr>), Tr::SMEM, attr_set);
+  if (e != cudaSuccess) return e;
   tc_gemm_kernel<Tr><<<grid, Tr::THREADS, Tr::SMEM, st>>>(a, b, p);
   return cudaGetLastError();
 }

@@ -126,8 +126,10 @@ CUCOSMA_API cucosma_status cucosma_gemm(const cucosma_gemm_desc* d, const void* 
 /* Reference-shaped FP32 / FP64 entry points: the compile-time M, N, K, ALPHA,
  * BETA of config.h become arguments (cuCOSMAV100.cuh:2774; the FP64 form is
  * the TYPE=double instantiation).  Native arithmetic, no epilogue; any split-K
- * workspace is library-managed (allocated once per device and grown on
- * demand, like the reference's internal cudaMalloc but not per call). */
+ * workspace is library-managed (allocated once per device and stream and
+ * grown on demand, like the reference's internal cudaMalloc but not per
+ * call), so the first split-K call on a stream must not be inside a stream
+ * capture. */
 CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
                              float beta, float* C, int ldc, void* stream);
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,

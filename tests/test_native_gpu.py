@@ -156,6 +156,30 @@ def test_tile_ids_in_plan(cuda):
         assert cc.get_plan(cc.make_desc(A, B, Cm, tile=1))["tile_m"] == 128
 
 
+def test_reference_entry_point_concurrent_streams(cuda):
+    """cucosma_sgemm's library-managed split-K workspace is per stream: two
+    split-K calls queued on two streams without any ordering between them
+    must both come out right (a shared workspace would mix their partials)."""
+    import torch
+
+    m, n, k = 100, 90, 30000
+    assert cc.get_plan(cc.make_desc(to_dev(np.zeros((m, k), np.float32)), to_dev(np.zeros((k, n), np.float32)),
+                                    to_dev(np.zeros((m, n), np.float32))))["splits"] > 1
+    cases = []
+    for seed in (60, 70):
+        A, B, Cin = uniform(seed, (m, k)), uniform(seed + 1, (k, n)), uniform(seed + 2, (m, n))
+        cases.append((A, B, Cin, to_dev(A), to_dev(B), to_dev(Cin)))
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for rep in range(3):
+        for (A, B, Cin, dA, dB, dC), st in zip(cases, streams):
+            with torch.cuda.stream(st):
+                cc.cosma_sgemm(dA, dB, dC, 1.0, 0.0 if rep else 0.5, stream=st)
+    torch.cuda.synchronize()
+    for A, B, Cin, dA, dB, dC in cases:
+        check_against_oracle(dC.cpu().numpy(), A, B, Cin, 1.0, 0.0, oracle.EPI_NONE, np.float32)
+
+
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "gemm_*.npz")))
 
 
