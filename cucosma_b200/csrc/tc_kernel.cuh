@@ -382,7 +382,12 @@ struct EpiF32 {
   static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
 
   // Stores the 32 x 32 block staged in stg (row r of the warp's rows in
-  // stg[r * 33 + ...]) at columns col0 + c0 + [0, 32): coalesced rows.
+  // stg[r * 33 + ...]) at columns col0 + c0 + [0, 32): coalesced rows.  When
+  // beta != 0 the C values of G rows are read together before those rows are
+  // written, so a block costs 32 / G read latencies instead of one a row (a
+  // store may alias the next row's read, so the reads are not reordered
+  // across the stores otherwise).  G trades registers for latency.
+  template <int G>
   static __device__ __forceinline__ void store32(const OutCtx& p, const float* stg, int lane, int row0, int col,
                                                  int z) {
     if (col >= p.n) return;
@@ -396,12 +401,17 @@ struct EpiF32 {
     } else {
       const float alpha = (float)p.alpha, beta = (float)p.beta;
       float* o = reinterpret_cast<float*>(p.out) + col;
-#pragma unroll 4
-      for (int r = 0; r < 32; ++r) {
-        const int row = row0 + r;
-        if (row < p.m) {
-          float* po = o + (int64_t)row * p.ldo;
-          *po = apply_epi(combine(stg[r * 33 + lane], alpha, beta, po), p.epilogue);
+#pragma unroll 1
+      for (int g = 0; g < 32; g += G) {
+        float c[G];
+#pragma unroll
+        for (int r = 0; r < G; ++r)
+          c[r] = beta != 0.f && row0 + g + r < p.m ? o[(int64_t)(row0 + g + r) * p.ldo] : 0.f;
+#pragma unroll
+        for (int r = 0; r < G; ++r) {
+          const int row = row0 + g + r;
+          if (row < p.m)
+            o[(int64_t)row * p.ldo] = apply_epi(combine(stg[(g + r) * 33 + lane], alpha, beta, &c[r]), p.epilogue);
         }
       }
     }
@@ -423,7 +433,7 @@ struct EpiF32 {
         stg[lane * 33 + 16 + j] = __uint_as_float(v1[j]);
       }
       __syncwarp();
-      store32(p, stg, lane, row0, col0 + c0 + lane, z);
+      store32<16>(p, stg, lane, row0, col0 + c0 + lane, z);
       __syncwarp();
     }
   }
@@ -461,7 +471,7 @@ struct EpiF32 {
 #pragma unroll
       for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = master[c0 + j];
       __syncwarp();
-      store32(p, stg, lane, row0, col0 + c0 + lane, z);
+      store32<8>(p, stg, lane, row0, col0 + c0 + lane, z);  // master[] holds most registers: 8 C rows at a time
       __syncwarp();
     }
   }
@@ -478,8 +488,10 @@ struct EpiOzaki {
   static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
                                              int col0, int z) {
     double* stg = reinterpret_cast<double*>(stg_raw);
+    const int cl = lane & 15;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
+      const int col = col0 + c0 + cl;
       double part[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) part[j] = 0.0;
@@ -495,11 +507,22 @@ struct EpiOzaki {
 #pragma unroll
       for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = part[j];
       __syncwarp();
-      const int cl = lane & 15;
-      const int col = col0 + c0 + cl;
       if (col < p.n) {
         const int ecol = p.partial ? 0 : p.eb[col];
-#pragma unroll 4
+        // This lane's 16 outputs (column col, rows (lane >> 4) + 2h): their row
+        // exponents and, when beta != 0, their C values, read together up
+        // front (the stores below may alias them, so they are not reordered
+        // otherwise): one read latency a chunk instead of one a row.
+        int erow[16];
+        double cv[16];
+#pragma unroll
+        for (int h = 0; h < 16; ++h) {
+          const int row = row0 + (lane >> 4) + 2 * h;
+          const bool in = !p.partial && row < p.m;
+          erow[h] = in ? p.ea[row] : 0;
+          cv[h] = in && p.beta != 0.0 ? reinterpret_cast<const double*>(p.out)[(int64_t)row * p.ldo + col] : 0.0;
+        }
+#pragma unroll
         for (int h = 0; h < 16; ++h) {
           const int r = (lane >> 4) + 2 * h;
           const int row = row0 + r;
@@ -509,8 +532,8 @@ struct EpiOzaki {
             reinterpret_cast<double*>(p.out)[(int64_t)z * p.ws_split_stride + (int64_t)row * p.ldo + col] = v;
           } else {
             double* po = reinterpret_cast<double*>(p.out) + (int64_t)row * p.ldo + col;
-            const double r_ = ldexp(v, p.ea[row] + ecol);
-            const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * *po);
+            const double r_ = ldexp(v, erow[h] + ecol);
+            const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * cv[h]);
             *po = apply_epi(o, p.epilogue);
           }
         }
