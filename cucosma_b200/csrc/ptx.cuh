@@ -88,6 +88,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int er
 }
 
 // ----------------------------------------------------------------------- TMA
+// Hint: bring the 128-byte line holding p into L2 (no data returned, no
+// register written).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<uint64_t>(p)));
+}
+
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* m) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(m)) : "memory");
 }

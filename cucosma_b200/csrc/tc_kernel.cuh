@@ -100,6 +100,27 @@ __device__ __forceinline__ void resolve_unit(const TcParams& p, const CUtensorMa
   }
 }
 
+// With beta != 0: L2 prefetch of the C block an epilogue warp will read
+// (rows row0 + [0, 32), columns col0 + [0, cols) of es-byte elements), issued
+// before the warp waits for the tile's accumulators so that the reads find
+// C in L2 instead of paying HBM latency inside the epilogue.  Every address
+// stays inside the m x n region (the last line of a row is clamped to its
+// last element).
+__device__ __forceinline__ void prefetch_c_block(const OutCtx& o, int row0, int col0, int cols, int es, int lane) {
+  if (o.partial || o.beta == 0.0 || col0 >= o.n) return;
+  const int c1 = min(o.n, col0 + cols);
+  const int lines = ((c1 - col0) * es + 127) / 128 + 1;  // rows need not start on a line
+  const char* base = static_cast<const char*>(o.out);
+  for (int i = lane; i < 32 * lines; i += 32) {
+    const int r = i / lines, l = i - r * lines;
+    const int row = row0 + r;
+    if (row >= o.m) continue;
+    const char* rowp = base + (int64_t)row * o.ldo * es;
+    const int64_t off = min((int64_t)col0 * es + (int64_t)l * 128, (int64_t)(c1 - 1) * es);
+    prefetch_l2(rowp + off);
+  }
+}
+
 __device__ __forceinline__ OutCtx out_ctx(const TcParams& p, const Unit& u) {
   OutCtx o;
   o.epilogue = p.epilogue;
@@ -336,6 +357,7 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
       const int z = u.z;
       const int row0 = u.tm * 128 + 32 * q;
       const int col0 = u.tn * BN;
+      prefetch_c_block(o, row0, col0 + (Tr::PROMOTE ? colsub : 0), Tr::PROMOTE ? W : BN, Tr::kInt8 ? 8 : 4, lane);
       if constexpr (Tr::PROMOTE) {
         float master[W];
 #pragma unroll
