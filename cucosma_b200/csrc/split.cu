@@ -230,6 +230,9 @@ __global__ void __launch_bounds__(256)
         for (int q = 0; q < 4; ++q) m = fmax(m, fabs(v[j][q]));
       }
     } else {
+      // long rows: four steps' loads in flight per thread (the row is read
+      // twice, so this pass and the slicing pass below stream from HBM)
+#pragma unroll 4
       for (int c = tid * 4; c < kpad; c += 1024) {
         double w[4];
         load4(src, c, cols, w);
@@ -254,6 +257,7 @@ __global__ void __launch_bounds__(256)
         if (c < kpad) store_slices4<S>(out, r, c, kpad, v[j], e);
       }
     } else {
+#pragma unroll 4
       for (int c = tid * 4; c < kpad; c += 1024) {
         double w[4];
         load4(src, c, cols, w);
