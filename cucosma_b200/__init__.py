@@ -54,7 +54,8 @@ class PlanInfo(C.Structure):
         ("splits", C.c_int32), ("band", C.c_int32), ("slices", C.c_int32), ("launches", C.c_int32),
         ("kchunk", C.c_int64), ("kpad", C.c_int64),
         ("workspace_bytes", C.c_uint64), ("off_a", C.c_uint64), ("off_b", C.c_uint64), ("off_ea", C.c_uint64),
-        ("off_eb", C.c_uint64), ("off_part", C.c_uint64),
+        ("off_eb", C.c_uint64), ("off_part", C.c_uint64), ("off_choice", C.c_uint64),
+        ("layout_slices", C.c_int32), ("reserved", C.c_int32),
     ]
 
     def as_dict(self):
@@ -68,6 +69,7 @@ EXPORTS = [
     "cucosma_gemm_desc_init", "cucosma_gemm_workspace_size", "cucosma_gemm", "cucosma_sgemm", "cucosma_dgemm",
     "cucosma_device_status", "cucosma_set_wait_timeout_ns", "cucosma_get_error_string", "cucosma_get_version",
     "cucosma_launch_count", "cucosma_profile_start", "cucosma_profile_stop", "cucosma_gemm_get_plan",
+    "cucosma_gemm_managed",
 ]
 
 
@@ -94,6 +96,7 @@ def lib():
     L.cucosma_launch_count.restype = C.c_ulonglong
     L.cucosma_profile_stop.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.cucosma_gemm_get_plan.argtypes = [C.POINTER(GemmDesc), C.POINTER(PlanInfo)]
+    L.cucosma_gemm_managed.argtypes = [C.POINTER(GemmDesc), vp, vp, vp, vp]
     for name in EXPORTS:
         if name not in ("cucosma_gemm_desc_init", "cucosma_get_error_string", "cucosma_get_version",
                         "cucosma_launch_count"):

@@ -115,7 +115,7 @@ cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B
   if (d->split_k < 0 || d->swizzle < 0) return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->flags != 0 && (d->flags != CUCOSMA_FLAG_TEST_SKIP_STAGE || d->precision == CUCOSMA_PRECISION_NATIVE))
     return CUCOSMA_STATUS_INVALID_VALUE;
-  if (d->slices != 0 && (d->slices < 4 || d->slices > 12)) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (d->slices != 0 && (d->slices < 4 || d->slices > 9)) return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->m == 0 || d->n == 0) return CUCOSMA_STATUS_SUCCESS;
   if (d->ldc < d->n) return CUCOSMA_STATUS_INVALID_VALUE;
   if (!C) return CUCOSMA_STATUS_INVALID_VALUE;
@@ -238,7 +238,8 @@ NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws) {
 // ---------------------------------------------------------------- dispatch
 template <typename T>
 static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& pl, const T* A, const T* B, T* C,
-                                 void* ws, const DeviceInfo* di, cudaStream_t st) {
+                                 void* ws, const DeviceInfo* di, cudaStream_t st, const int* gate = nullptr,
+                                 int gate_value = 0, bool profile = true) {
   constexpr int BK = simt::Cfg<T>::BK;
   const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
   CUtensorMap tmA, tmB;
@@ -258,6 +259,8 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
   p.epilogue = d->epilogue;
   p.alpha = d->alpha;
   p.beta = d->beta;
+  p.gate = gate;
+  p.gate_value = gate_value;
   wait_ctl(di, &p.ctl.status, &p.ctl.timeout_ns);
   if (pl.splits > 1) {
     p.partial = 1;
@@ -269,16 +272,25 @@ static cucosma_status run_native(const cucosma_gemm_desc* d, const NativePlan& p
     p.out = C;
     p.ldo = d->ldc;
   }
-  prof_begin(st);
+  if (profile) prof_begin(st);
   if (simt::launch_gemm<T>(tmA, tmB, p, pl.bm, st) != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
-  prof_end(st);
+  if (profile) prof_end(st);
   note_launches(pl.splits > 1 ? 2 : 1);
   if (pl.splits > 1) {
     if (simt::launch_reduce<T>(static_cast<const T*>(ws), p.ws_split_stride, pl.ldw, pl.splits, C, d->ldc, p.m, p.n,
-                               d->alpha, d->beta, d->epilogue, di->sms, st) != cudaSuccess)
+                               d->alpha, d->beta, d->epilogue, di->sms, st, gate, gate_value) != cudaSuccess)
       return CUCOSMA_STATUS_LAUNCH_FAILED;
   }
   return CUCOSMA_STATUS_SUCCESS;
+}
+
+cucosma_status native_gemm_gated(const cucosma_gemm_desc* d, const NativePlan& pl, const void* A, const void* B,
+                                 void* C, void* ws, const DeviceInfo* di, cudaStream_t st, const int* gate,
+                                 int gate_value) {
+  if (d->dtype == CUCOSMA_R_32F)
+    return run_native<float>(d, pl, (const float*)A, (const float*)B, (float*)C, ws, di, st, gate, gate_value, false);
+  return run_native<double>(d, pl, (const double*)A, (const double*)B, (double*)C, ws, di, st, gate, gate_value,
+                            false);
 }
 
 // Skinny-shape kernels (skinny.cu) for native precision: tiny K, or tiny M or N.
@@ -313,6 +325,11 @@ cucosma_status workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const D
 
 cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,
                     cudaStream_t st) {
+  return gemm_ex(d, A, B, C, ws, ws_bytes, st, kPrepA | kPrepB);
+}
+
+cucosma_status gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,
+                       cudaStream_t st, int prep) {
   cucosma_status s = validate(d, A, B, C);
   if (s != CUCOSMA_STATUS_SUCCESS) return s;
   if (d->m == 0 || d->n == 0) return CUCOSMA_STATUS_SUCCESS;
@@ -344,7 +361,7 @@ cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, vo
     return fp32 ? run_native<float>(d, pl, (const float*)A, (const float*)B, (float*)C, ws, di, st)
                 : run_native<double>(d, pl, (const double*)A, (const double*)B, (double*)C, ws, di, st);
   }
-  return tc_gemm(d, A, B, C, ws, di, st);
+  return tc_gemm_ex(d, A, B, C, ws, di, st, prep);
 }
 
 // ---------------------------------------------- launch count and profiling
@@ -387,6 +404,10 @@ void* managed_workspace(size_t bytes, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(mu);
   auto& slot = slots[{dev, st}];
   if (slot.second < bytes) {
+    // Allocating (and the synchronisation before freeing) would break a
+    // stream capture: refuse instead.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return nullptr;
     if (slot.first) {
       cudaStreamSynchronize(st);  // the old buffer may still be in use by queued work
       cudaFree(slot.first);
@@ -475,6 +496,21 @@ extern "C" cucosma_status cucosma_gemm(const cucosma_gemm_desc* d, const void* A
   return gemm(d, A, B, C, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
+extern "C" cucosma_status cucosma_gemm_managed(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
+                                               void* stream) {
+  cucosma_status s = validate(d, A, B, C);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  size_t need = 0;
+  s = cucosma_gemm_workspace_size(d, &need);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  void* ws = nullptr;
+  if (need) {
+    ws = managed_workspace(need, static_cast<cudaStream_t>(stream));
+    if (!ws) return CUCOSMA_STATUS_ALLOC_FAILED;
+  }
+  return gemm(d, A, B, C, ws, need, static_cast<cudaStream_t>(stream));
+}
+
 template <typename T>
 static cucosma_status plain_gemm(int dtype, int m, int n, int k, T alpha, const T* A, int lda, const T* B, int ldb,
                                  T beta, T* C, int ldc, void* stream) {
@@ -489,17 +525,7 @@ static cucosma_status plain_gemm(int dtype, int m, int n, int k, T alpha, const 
   d.dtype = dtype;
   d.alpha = alpha;
   d.beta = beta;
-  cucosma_status s = validate(&d, A, B, C);
-  if (s != CUCOSMA_STATUS_SUCCESS) return s;
-  size_t need = 0;
-  s = cucosma_gemm_workspace_size(&d, &need);
-  if (s != CUCOSMA_STATUS_SUCCESS) return s;
-  void* ws = nullptr;
-  if (need) {
-    ws = managed_workspace(need, static_cast<cudaStream_t>(stream));
-    if (!ws) return CUCOSMA_STATUS_ALLOC_FAILED;
-  }
-  return gemm(&d, A, B, C, ws, need, static_cast<cudaStream_t>(stream));
+  return cucosma_gemm_managed(&d, A, B, C, stream);
 }
 
 extern "C" cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const float* A, int lda, const float* B,

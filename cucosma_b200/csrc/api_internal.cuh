@@ -19,6 +19,9 @@ struct WaitCtl;
 // Wait control for launches on the current device.
 void wait_ctl(const DeviceInfo* di, int** status, unsigned long long* timeout_ns);
 
+// Operand pre-passes of the tensor-core paths (see tc_gemm_ex).
+enum : int { kPrepA = 1, kPrepB = 2 };
+
 struct NativePlan {
   int bm;  // CTA tile rows: 128, or 64 (FP32 only); 128 columns either way
   int tiles_m, tiles_n, splits, swizzle;
@@ -32,6 +35,10 @@ NativePlan plan_native(const cucosma_gemm_desc* d, int sms, size_t max_ws = SIZE
 cucosma_status validate(const cucosma_gemm_desc* d, const void* A, const void* B, const void* C);
 cucosma_status gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,
                     cudaStream_t st);
+// The same with a choice of operand pre-passes for the tensor-core paths
+// (kPrepA / kPrepB; the native paths have none).
+cucosma_status gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws, size_t ws_bytes,
+                       cudaStream_t st, int prep);
 
 bool encode_2d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const void* base, uint64_t inner,
                uint64_t outer, uint64_t row_stride_elems, uint32_t box_inner, uint32_t box_outer,
@@ -45,10 +52,20 @@ cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, cons
 void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info);
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                        const DeviceInfo* di, cudaStream_t st);
-// BF16 paths only: planes_ready = true skips the split pre-pass (the caller
-// has written the operand planes at the plan's offsets in ws).
+// prep: which operand pre-passes run (kPrepA | kPrepB for a plain call).  An
+// operand left out must already be in ws at the plan's offsets -- written by
+// the caller (the backward pass), or by an earlier call on the same B (row
+// blocks of one problem: B's planes / slices, exponents and magnitude sums
+// sit first in the workspace and depend on N, K and the slice layout only).
 cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
-                          const DeviceInfo* di, cudaStream_t st, bool planes_ready);
+                          const DeviceInfo* di, cudaStream_t st, int prep);
+
+// The native tile kernel (no skinny-shape kernels) with plan pl; with a gate
+// every kernel it enqueues runs only if *gate == gate_value on the device.
+// Counts its launches; does not take part in the main-kernel profiling.
+cucosma_status native_gemm_gated(const cucosma_gemm_desc* d, const NativePlan& pl, const void* A, const void* B,
+                                 void* C, void* ws, const DeviceInfo* di, cudaStream_t st, const int* gate,
+                                 int gate_value);
 
 void* managed_workspace(size_t bytes, cudaStream_t st);
 

@@ -106,31 +106,42 @@ extern "C" cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* f, cons
   const float* fY = static_cast<const float*>(Y);
   const float* fdY = static_cast<const float*>(dY);
   cucosma_plan_info pi;
+  // Each product's descriptor is resolved against the tuning cache once and
+  // that one descriptor gives both the plan (plane offsets, partials region)
+  // and the launch, so the two cannot disagree; the plan must fit the
+  // caller's workspace (the cache may have changed since it was sized).
+  auto resolve = [&](cucosma_gemm_desc* d, cucosma_gemm_desc* tuned) -> const cucosma_gemm_desc* {
+    const cucosma_gemm_desc* r = apply_tuning(d, tuned, di);
+    tc_plan_info(r, di, &pi);
+    return r;
+  };
   if (dA) {
     // dA (m x k) = G (m x n) * B^T: K' = n.
-    cucosma_gemm_desc d;
-    sub_desc(f, m, k, n, ldda, &d);
-    if ((s = cucosma_gemm_get_plan(&d, &pi)) != CUCOSMA_STATUS_SUCCESS) return s;
+    cucosma_gemm_desc d0, tuned;
+    sub_desc(f, m, k, n, ldda, &d0);
+    const cucosma_gemm_desc* d = resolve(&d0, &tuned);
+    if (pi.workspace_bytes > workspace_bytes) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
     if (launch_split_bf16(fdY, lddy, (int)m, (int)n, pi.kpad, nt, w + pi.off_a, false, di->sms, st, xf, fY, ldy,
                           scale) != cudaSuccess ||
         launch_split_bf16(static_cast<const float*>(B), f->ldb, (int)k, (int)n, pi.kpad, nt, w + pi.off_b, false,
                           di->sms, st) != cudaSuccess)
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     note_launches(2);
-    if ((s = tc_gemm_ex(&d, nullptr, nullptr, dA, workspace, di, st, true)) != CUCOSMA_STATUS_SUCCESS) return s;
+    if ((s = tc_gemm_ex(d, nullptr, nullptr, dA, workspace, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
   }
   if (dB) {
     // dB (k x n) = A^T (k x m) * G (m x n): K' = m.
-    cucosma_gemm_desc d;
-    sub_desc(f, k, n, m, lddb, &d);
-    if ((s = cucosma_gemm_get_plan(&d, &pi)) != CUCOSMA_STATUS_SUCCESS) return s;
+    cucosma_gemm_desc d0, tuned;
+    sub_desc(f, k, n, m, lddb, &d0);
+    const cucosma_gemm_desc* d = resolve(&d0, &tuned);
+    if (pi.workspace_bytes > workspace_bytes) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
     if (launch_split_bf16(static_cast<const float*>(A), f->lda, (int)m, (int)k, pi.kpad, nt, w + pi.off_a, true,
                           di->sms, st) != cudaSuccess ||
         launch_split_bf16(fdY, lddy, (int)m, (int)n, pi.kpad, nt, w + pi.off_b, true, di->sms, st, xf, fY, ldy,
                           scale) != cudaSuccess)
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     note_launches(2);
-    if ((s = tc_gemm_ex(&d, nullptr, nullptr, dB, workspace, di, st, true)) != CUCOSMA_STATUS_SUCCESS) return s;
+    if ((s = tc_gemm_ex(d, nullptr, nullptr, dB, workspace, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
   }
   return CUCOSMA_STATUS_SUCCESS;
 }

@@ -3,6 +3,8 @@
 #pragma once
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cuda_runtime.h>
 
 #include "ptx.cuh"
@@ -21,6 +23,14 @@ inline cudaError_t ensure_smem_attr(const void* fn, int bytes, std::atomic<uint6
   if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+  return e;
+}
+
+// With CUCOSMA_DEBUG set in the environment, a failing CUDA call inside the
+// library is reported on stderr (the C ABI itself only returns a status).
+inline cudaError_t debug_cuda(const char* what, cudaError_t e) {
+  static const bool on = std::getenv("CUCOSMA_DEBUG") != nullptr;
+  if (e != cudaSuccess && on) std::fprintf(stderr, "cucosma: %s: %s\n", what, cudaGetErrorString(e));
   return e;
 }
 

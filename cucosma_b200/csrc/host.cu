@@ -4,12 +4,16 @@
 // themselves around cosmaSgemm (test_correctness.h).  The caller's device
 // buffer holds device copies of A, B and C and the GEMM workspace.  B goes
 // over first; A (and C when beta != 0) follow in row blocks, each block's
-// GEMM (a row slice of the problem through the regular entry point) runs as
-// soon as its rows have arrived, and its C rows go back while later blocks
-// still copy in -- so the host-to-device and device-to-host transfers run
-// concurrently with each other and with the compute.  Three streams per
-// device (created on first use) carry the copies in, the GEMMs and the copies
-// out; the caller's stream waits for the last copy out.
+// GEMM (a row slice of the problem) runs as soon as its rows have arrived,
+// and its C rows go back while later blocks still copy in -- so the
+// host-to-device and device-to-host transfers run concurrently with each
+// other and with the compute.  On the tensor-core paths B's operand planes
+// (BF16 split or Ozaki slices, with its exponents) are prepared once, by the
+// first block, and reused by the others.  Three streams per device (created
+// on first use) carry the copies in, the GEMMs and the copies out; the
+// events that order them are created for each call, so calls from several
+// host threads never share one.  The caller's stream waits for the last
+// copy out.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -25,9 +29,29 @@ constexpr int kMaxBlocks = 16;
 
 struct HostStreams {
   cudaStream_t in = nullptr, gemm = nullptr, out = nullptr;
+  bool ok = false;
+};
+
+// The events of one call (destroyed when the call returns; CUDA releases an
+// event that is still pending once its work completes).
+struct CallEvents {
   cudaEvent_t start = nullptr, b_in = nullptr, done = nullptr;
   cudaEvent_t a_in[kMaxBlocks] = {}, c_ready[kMaxBlocks] = {};
-  bool ok = false;
+  bool create(int blocks) {
+    auto mk = [](cudaEvent_t* e) { return cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess; };
+    if (!mk(&start) || !mk(&b_in) || !mk(&done)) return false;
+    for (int i = 0; i < blocks; ++i)
+      if (!mk(&a_in[i]) || !mk(&c_ready[i])) return false;
+    return true;
+  }
+  ~CallEvents() {
+    for (cudaEvent_t e : {start, b_in, done})
+      if (e) cudaEventDestroy(e);
+    for (int i = 0; i < kMaxBlocks; ++i) {
+      if (a_in[i]) cudaEventDestroy(a_in[i]);
+      if (c_ready[i]) cudaEventDestroy(c_ready[i]);
+    }
+  }
 };
 
 HostStreams* streams_for_current_device() {
@@ -38,15 +62,9 @@ HostStreams* streams_for_current_device() {
   std::lock_guard<std::mutex> lock(mu);
   HostStreams& h = per_device[dev];
   if (!h.ok) {
-    bool good = cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking) == cudaSuccess &&
-                cudaStreamCreateWithFlags(&h.gemm, cudaStreamNonBlocking) == cudaSuccess &&
-                cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking) == cudaSuccess &&
-                cudaEventCreateWithFlags(&h.start, cudaEventDisableTiming) == cudaSuccess &&
-                cudaEventCreateWithFlags(&h.b_in, cudaEventDisableTiming) == cudaSuccess &&
-                cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) == cudaSuccess;
-    for (int i = 0; good && i < kMaxBlocks; ++i)
-      good = cudaEventCreateWithFlags(&h.a_in[i], cudaEventDisableTiming) == cudaSuccess &&
-             cudaEventCreateWithFlags(&h.c_ready[i], cudaEventDisableTiming) == cudaSuccess;
+    const bool good = cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking) == cudaSuccess &&
+                      cudaStreamCreateWithFlags(&h.gemm, cudaStreamNonBlocking) == cudaSuccess &&
+                      cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking) == cudaSuccess;
     if (!good) return nullptr;
     h.ok = true;
   }
@@ -127,6 +145,8 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
   if (reinterpret_cast<uintptr_t>(device_buffer) & 255) return CUCOSMA_STATUS_MISALIGNED;
   HostStreams* h = streams_for_current_device();
   if (!h) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  CallEvents ev;
+  if (!ev.create(L.blocks)) return CUCOSMA_STATUS_LAUNCH_FAILED;
   const size_t es = d->dtype == CUCOSMA_R_32F ? 4 : 8;
   uint8_t* w = static_cast<uint8_t*>(device_buffer);
   uint8_t* dA = w + L.off_a;
@@ -140,11 +160,11 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
   auto fail = [](cudaError_t e) { return e != cudaSuccess; };
 
   // Everything starts after the work already queued on the caller's stream.
-  if (fail(cudaEventRecord(h->start, caller)) || fail(cudaStreamWaitEvent(h->in, h->start, 0)) ||
-      fail(cudaStreamWaitEvent(h->gemm, h->start, 0)) || fail(cudaStreamWaitEvent(h->out, h->start, 0)))
+  if (fail(cudaEventRecord(ev.start, caller)) || fail(cudaStreamWaitEvent(h->in, ev.start, 0)) ||
+      fail(cudaStreamWaitEvent(h->gemm, ev.start, 0)) || fail(cudaStreamWaitEvent(h->out, ev.start, 0)))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (fail(cudaMemcpy2DAsync(dB, L.ldb * es, hB, d->ldb * es, d->n * es, d->k, cudaMemcpyHostToDevice, h->in)) ||
-      fail(cudaEventRecord(h->b_in, h->in)) || fail(cudaStreamWaitEvent(h->gemm, h->b_in, 0)))
+      fail(cudaEventRecord(ev.b_in, h->in)) || fail(cudaStreamWaitEvent(h->gemm, ev.b_in, 0)))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   for (int i = 0; i < L.blocks; ++i) {
     const int64_t r0 = i * L.rows_per_block, rows = std::min<int64_t>(L.rows_per_block, d->m - r0);
@@ -155,21 +175,23 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
         fail(cudaMemcpy2DAsync(dC + r0 * L.ldc * es, L.ldc * es, hC + r0 * d->ldc * es, d->ldc * es, d->n * es, rows,
                                cudaMemcpyHostToDevice, h->in)))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
-    if (fail(cudaEventRecord(h->a_in[i], h->in)) || fail(cudaStreamWaitEvent(h->gemm, h->a_in[i], 0)))
+    if (fail(cudaEventRecord(ev.a_in[i], h->in)) || fail(cudaStreamWaitEvent(h->gemm, ev.a_in[i], 0)))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     cucosma_gemm_desc sub = *d;
     sub.m = rows;
     sub.lda = L.lda;
     sub.ldb = L.ldb;
     sub.ldc = L.ldc;
-    s = cucosma_gemm(&sub, dA + r0 * L.lda * es, dB, dC + r0 * L.ldc * es, ws, L.ws_bytes, h->gemm);
+    // B's operand planes: prepared by the first block, reused by the rest.
+    s = gemm_ex(&sub, dA + r0 * L.lda * es, dB, dC + r0 * L.ldc * es, ws, L.ws_bytes, h->gemm,
+                i == 0 ? (kPrepA | kPrepB) : kPrepA);
     if (s != CUCOSMA_STATUS_SUCCESS) return s;
-    if (fail(cudaEventRecord(h->c_ready[i], h->gemm)) || fail(cudaStreamWaitEvent(h->out, h->c_ready[i], 0)) ||
+    if (fail(cudaEventRecord(ev.c_ready[i], h->gemm)) || fail(cudaStreamWaitEvent(h->out, ev.c_ready[i], 0)) ||
         fail(cudaMemcpy2DAsync(hC + r0 * d->ldc * es, d->ldc * es, dC + r0 * L.ldc * es, L.ldc * es, d->n * es, rows,
                                cudaMemcpyDeviceToHost, h->out)))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
   }
-  if (fail(cudaEventRecord(h->done, h->out)) || fail(cudaStreamWaitEvent(caller, h->done, 0)))
+  if (fail(cudaEventRecord(ev.done, h->out)) || fail(cudaStreamWaitEvent(caller, ev.done, 0)))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   return CUCOSMA_STATUS_SUCCESS;
 }

@@ -86,7 +86,7 @@ extern "C" cucosma_status cucosma_sgemm_splitk_static(int m, int n, int k, float
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   CUtensorMap tmA, tmB;
   constexpr int BK = simt::Cfg<float>::BK;
-  if (!encode_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, lda, BK, pl.bm, CU_TENSOR_MAP_SWIZZLE_64B))
+  if (!encode_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, lda, BK, pl.bm, simt::Cfg<float>::A_SWIZZLE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (!encode_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, ldb, simt::BN, BK, CU_TENSOR_MAP_SWIZZLE_NONE))
     return CUCOSMA_STATUS_LAUNCH_FAILED;

@@ -88,6 +88,7 @@ template <int BM_>
 __global__ void __launch_bounds__(simt::SgemmShape<BM_>::kThreads, simt::SgemmShape<BM_>::kCtasPerSm)
     simt_sgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const SimtParams p) {
+  if (p.gate != nullptr && *p.gate != p.gate_value) return;  // path not chosen on the device
   using namespace simt;
   using Shape = SgemmShape<BM_>;
   constexpr int BM = BM_, STAGES = Shape::kStages, kLdT = Shape::kLdT;
@@ -261,6 +262,7 @@ __device__ __forceinline__ void store_pair(const SimtParams& p, int r, int c, do
 __global__ void __launch_bounds__(simt::kThreads, 1)
     simt_dgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const SimtParams p) {
+  if (p.gate != nullptr && *p.gate != p.gate_value) return;  // path not chosen on the device
   using namespace simt;
   constexpr int BK = Cfg<double>::BK;  // 16
   constexpr int S = kDStages;
@@ -387,7 +389,9 @@ __global__ void __launch_bounds__(simt::kThreads, 1)
 // z ascending, the sum accumulated in T (cosmaSplitKReduce.cuh:31-40).
 template <typename T>
 __global__ void splitk_reduce_kernel(const T* __restrict__ ws, int64_t split_stride, int64_t ldw, int splits, T* C,
-                                     int64_t ldc, int m, int n, double alpha_d, double beta_d, int epi) {
+                                     int64_t ldc, int m, int n, double alpha_d, double beta_d, int epi,
+                                     const int* gate, int gate_value) {
+  if (gate != nullptr && *gate != gate_value) return;  // path not chosen on the device
   constexpr int VEC = Vec<T>::n;
   using V = typename Vec<T>::type;
   const T alpha = (T)alpha_d, beta = (T)beta_d;
@@ -500,14 +504,15 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Si
 
 template <typename T>
 cudaError_t launch_reduce(const T* ws, int64_t split_stride, int64_t ldw, int splits, T* C, int64_t ldc, int m, int n,
-                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream) {
+                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream, const int* gate,
+                          int gate_value) {
   const int64_t work = (int64_t)m * ceil_div(n, Vec<T>::n);
   const int threads = 256;
   int64_t blocks = ceil_div(work, threads);
   blocks = std::min<int64_t>(blocks, (int64_t)num_sms * 8);
   if (blocks < 1) blocks = 1;
   splitk_reduce_kernel<T><<<(unsigned)blocks, threads, 0, stream>>>(ws, split_stride, ldw, splits, C, ldc, m, n, alpha,
-                                                                    beta, epi);
+                                                                    beta, epi, gate, gate_value);
   return cudaGetLastError();
 }
 
@@ -537,9 +542,9 @@ template int occupancy<double>(int);
 template cudaError_t launch_gemm<float>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, int, cudaStream_t);
 template cudaError_t launch_gemm<double>(const CUtensorMap&, const CUtensorMap&, const SimtParams&, int, cudaStream_t);
 template cudaError_t launch_reduce<float>(const float*, int64_t, int64_t, int, float*, int64_t, int, int, double, double,
-                                          int, int, cudaStream_t);
+                                          int, int, cudaStream_t, const int*, int);
 template cudaError_t launch_reduce<double>(const double*, int64_t, int64_t, int, double*, int64_t, int, int, double,
-                                           double, int, int, cudaStream_t);
+                                           double, int, int, cudaStream_t, const int*, int);
 template cudaError_t launch_scale<float>(float*, int64_t, int, int, double, int, int, cudaStream_t);
 template cudaError_t launch_scale<double>(double*, int64_t, int, int, double, int, int, cudaStream_t);
 template size_t smem_bytes<float>(int);

@@ -22,6 +22,11 @@ struct SimtParams {
   int64_t ldo;            // row stride of out (elements)
   int64_t ws_split_stride;  // elements between consecutive splits in the workspace
   WaitCtl ctl;
+  // Optional device-side gate: when gate is set the kernel runs only if
+  // *gate == gate_value (a path chosen on the device, e.g. the adaptive
+  // Ozaki call's native FP64 fallback), and returns at once otherwise.
+  const int* gate;
+  int gate_value;
 };
 
 namespace simt {
@@ -74,7 +79,8 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Si
                         cudaStream_t stream);
 template <typename T>
 cudaError_t launch_reduce(const T* ws, int64_t split_stride, int64_t ldw, int splits, T* C, int64_t ldc, int m, int n,
-                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream);
+                          double alpha, double beta, int epi, int num_sms, cudaStream_t stream,
+                          const int* gate = nullptr, int gate_value = 0);
 template <typename T>
 cudaError_t launch_scale(T* C, int64_t ldc, int m, int n, double beta, int epi, int num_sms, cudaStream_t stream);
 }  // namespace simt

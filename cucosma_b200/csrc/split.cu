@@ -173,8 +173,9 @@ __global__ void __launch_bounds__(256)
 // columns per thread and step, two 16-byte loads), the maximum is reduced
 // across the block, and the slices are cut from the registers; longer rows
 // take a second pass over the row for the slices.  A thread's 4 columns give
-// one 4-byte store per slice.  Also finishes B's column exponents
-// (sentinel -> 0).
+// one 4-byte store per slice.  With stats, also the row's magnitude sum
+// sum_k floor(|a_rk| 2^(30 - e_r)) (integer, so exact and order-free) enters
+// stats->min_row by atomicMin (zero rows stay out).
 constexpr int kRowSteps = 8;                    // steps of 1024 columns held in registers
 constexpr int kRowRegK = kRowSteps * 1024;
 
@@ -206,10 +207,9 @@ __device__ __forceinline__ void store_slices4(int8_t* __restrict__ out, int64_t 
 template <int S>
 __global__ void __launch_bounds__(256)
     ozaki_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
-                      int32_t* __restrict__ ea, int8_t* __restrict__ out, int32_t* __restrict__ eb, int ncols) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncols; i += gridDim.x * blockDim.x)
-    if (eb[i] == kExpSentinel) eb[i] = 0;
+                      int32_t* __restrict__ ea, int8_t* __restrict__ out, OzakiStats* __restrict__ stats) {
   __shared__ double red[8];
+  __shared__ unsigned long long red_sum[8];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool in_regs = kpad <= kRowRegK;
   for (int r = blockIdx.x; r < rows; r += gridDim.x) {
@@ -250,11 +250,15 @@ __global__ void __launch_bounds__(256)
     __syncthreads();  // red is reused by the next row
     const int e = exp_of(m);
     if (tid == 0) ea[r] = e;
+    unsigned long long sum = 0;
     if (in_regs) {
 #pragma unroll
       for (int j = 0; j < kRowSteps; ++j) {
         const int c = (tid + 256 * j) * 4;
-        if (c < kpad) store_slices4<S>(out, r, c, kpad, v[j], e);
+        if (c < kpad) {
+          store_slices4<S>(out, r, c, kpad, v[j], e);
+          if (stats) sum += magnitude_fx4(v[j], e);
+        }
       }
     } else {
 #pragma unroll 4
@@ -262,7 +266,21 @@ __global__ void __launch_bounds__(256)
         double w[4];
         load4(src, c, cols, w);
         store_slices4<S>(out, r, c, kpad, w, e);
+        if (stats) sum += magnitude_fx4(w, e);
       }
+    }
+    if (stats) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0) red_sum[warp] = sum;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += red_sum[w];
+        if (t > 0) atomicMin(&stats->min_row, t);
+      }
+      __syncthreads();  // red_sum is reused by the next row
     }
   }
 }
@@ -272,10 +290,15 @@ __global__ void __launch_bounds__(256)
 // Stores: a lane slices 4 consecutive k of one column into one 4-byte store
 // per slice; 8 lanes cover a column's 32 bytes and a warp 4 adjacent columns
 // (128 contiguous bytes per slice).
+// Also finishes the column exponents (the blocks of the first k-tile turn
+// the all-zero columns' sentinel into exp_of(0) = 0; every block reads the
+// sentinel as 0) and, with colsum, adds each column's fixed-point magnitude
+// sum sum_k floor(|b_kn| 2^(30 - e_n)) by integer atomics (exact, so the
+// totals do not depend on the order of the blocks).
 template <int S>
 __global__ void __launch_bounds__(256)
     ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
-                            const int32_t* __restrict__ eb, int8_t* __restrict__ out) {
+                            int32_t* __restrict__ eb, int8_t* __restrict__ out, unsigned long long* __restrict__ colsum) {
   __shared__ double tile[32][65];
   const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 64, t = threadIdx.x;
 #pragma unroll
@@ -302,16 +325,63 @@ __global__ void __launch_bounds__(256)
   for (int p = 0; p < 2; ++p) {
     const int item = p * 256 + t, nl = item / 8, kq = item % 8;
     const int n = n0 + nl, k = k0 + kq * 4;
-    if (n >= ncols) continue;
-    const int e = eb[n];
-    int8_t q[4][S];
+    unsigned long long part = 0;
+    if (n < ncols) {
+      int e = eb[n];
+      if (e == kExpSentinel) {
+        e = 0;
+        if (blockIdx.y == 0 && kq == 0) eb[n] = 0;
+      }
+      double v[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) slice_value<S>(tile[kq * 4 + j][nl], e, q[j]);
+      for (int j = 0; j < 4; ++j) v[j] = tile[kq * 4 + j][nl];
+      int8_t q[4][S];
 #pragma unroll
-    for (int s_ = 0; s_ < S; ++s_) {
-      const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
-                          ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
-      *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, ncols, s_)) = pk;
+      for (int j = 0; j < 4; ++j) slice_value<S>(v[j], e, q[j]);
+#pragma unroll
+      for (int s_ = 0; s_ < S; ++s_) {
+        const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
+                            ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
+        *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, ncols, s_)) = pk;
+      }
+      if (colsum) part = magnitude_fx4(v, e);
+    }
+    if (colsum) {
+      // the 8 lanes of a column are consecutive: reduce over them
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if (kq == 0 && n < ncols && part) atomicAdd(&colsum[n], part);
+    }
+  }
+}
+
+// Minimum of the column magnitude sums over the nonzero columns into
+// stats->min_col; the last block to finish then makes the path choice (see
+// ozaki_choice) from both minima.
+__global__ void __launch_bounds__(256) ozaki_decide_kernel(const unsigned long long* __restrict__ colsum, int ncols,
+                                                           int64_t k, OzakiStats* stats) {
+  __shared__ unsigned long long red[8];
+  unsigned long long m = ~0ull;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncols; i += gridDim.x * blockDim.x) {
+    const unsigned long long v = colsum[i];
+    if (v != 0 && v < m) m = v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
+    m = w < m ? w : m;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < 8; ++w) m = red[w] < m ? red[w] : m;
+    if (m != ~0ull) atomicMin(&stats->min_col, m);
+    __threadfence();
+    const unsigned prev = atomicAdd(&stats->done_blocks, 1u);
+    if (prev == gridDim.x - 1) {
+      __threadfence();
+      const unsigned long long mr = atomicAdd(&stats->min_row, 0ull), mc = atomicAdd(&stats->min_col, 0ull);
+      stats->choice = ozaki_choice(mr, mc, k);
     }
   }
 }
@@ -360,42 +430,70 @@ cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, i
   return cudaGetLastError();
 }
 
-cudaError_t launch_ozaki_exponents(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                                   int32_t* ea, int32_t* eb, int sms, cudaStream_t st) {
-  // Row exponents of A are found by ozaki_rows_kernel (launch_ozaki_slices).
-  (void)A, (void)lda, (void)m, (void)ea, (void)sms;
-  cudaError_t e = cudaMemsetAsync(eb, 0x80, (size_t)n * sizeof(int32_t), st);
-  if (e != cudaSuccess) return e;
-  if (k > 0) {
-    const dim3 grid((unsigned)ceil_div(n, 512), (unsigned)ceil_div(k, 64));
-    ozaki_col_exp_kernel<<<grid, 256, 0, st>>>(B, ldb, k, n, eb);
-  }
+template <int S>
+static cudaError_t prep_b_s(const double* B, int64_t ldb, int k, int n, int64_t kpad, int32_t* eb, int8_t* sb,
+                            unsigned long long* colsum, cudaStream_t st) {
+  dim3 grid((unsigned)ceil_div(n, 64), (unsigned)ceil_div(kpad, 32));
+  ozaki_slice_cols_kernel<S><<<grid, 256, 0, st>>>(B, ldb, k, n, kpad, eb, sb, colsum);
   return cudaGetLastError();
 }
 
 template <int S>
-static cudaError_t slices_s(const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                            int64_t kpad, int32_t* ea, int32_t* eb, int8_t* sa, int8_t* sb, int sms,
-                            cudaStream_t st) {
+static cudaError_t prep_a_s(const double* A, int64_t lda, int m, int k, int64_t kpad, int32_t* ea, int8_t* sa,
+                            OzakiStats* stats, int sms, cudaStream_t st) {
   const unsigned rows_grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(m, (int64_t)sms * 8));
-  ozaki_rows_kernel<S><<<rows_grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, eb, n);
-  dim3 grid((unsigned)ceil_div(n, 64), (unsigned)ceil_div(kpad, 32));
-  ozaki_slice_cols_kernel<S><<<grid, 256, 0, st>>>(B, ldb, k, n, kpad, eb, sb);
+  ozaki_rows_kernel<S><<<rows_grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, stats);
   return cudaGetLastError();
 }
 
-cudaError_t launch_ozaki_slices(int s, const double* A, int64_t lda, const double* B, int64_t ldb, int m, int n, int k,
-                                int64_t kpad, int32_t* ea, int32_t* eb, int8_t* sa, int8_t* sb, int sms,
-                                cudaStream_t st) {
+cudaError_t launch_ozaki_prep_b(int s, const double* B, int64_t ldb, int k, int n, int64_t kpad, int32_t* eb,
+                                int8_t* sb, unsigned long long* colsum, OzakiStats* stats, int sms, cudaStream_t st) {
+  (void)sms;
+  cudaError_t e = cudaMemsetAsync(eb, 0x80, (size_t)n * sizeof(int32_t), st);
+  if (e == cudaSuccess && colsum) e = cudaMemsetAsync(colsum, 0, (size_t)n * sizeof(unsigned long long), st);
+  if (e == cudaSuccess && stats) e = cudaMemsetAsync(&stats->min_col, 0xFF, sizeof(stats->min_col), st);
+  if (e != cudaSuccess) return e;
+  if (k > 0) {
+    const dim3 grid((unsigned)ceil_div(n, 512), (unsigned)ceil_div(k, 64));
+    ozaki_col_exp_kernel<<<grid, 256, 0, st>>>(B, ldb, k, n, eb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   switch (s) {
-    case 4: return slices_s<4>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
-    case 5: return slices_s<5>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
-    case 6: return slices_s<6>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
-    case 7: return slices_s<7>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
-    case 8: return slices_s<8>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
-    case 9: return slices_s<9>(A, lda, B, ldb, m, n, k, kpad, ea, eb, sa, sb, sms, st);
+    case 4: return prep_b_s<4>(B, ldb, k, n, kpad, eb, sb, colsum, st);
+    case 5: return prep_b_s<5>(B, ldb, k, n, kpad, eb, sb, colsum, st);
+    case 6: return prep_b_s<6>(B, ldb, k, n, kpad, eb, sb, colsum, st);
+    case 7: return prep_b_s<7>(B, ldb, k, n, kpad, eb, sb, colsum, st);
+    case 8: return prep_b_s<8>(B, ldb, k, n, kpad, eb, sb, colsum, st);
+    case 9: return prep_b_s<9>(B, ldb, k, n, kpad, eb, sb, colsum, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_ozaki_prep_a(int s, const double* A, int64_t lda, int m, int k, int64_t kpad, int32_t* ea,
+                                int8_t* sa, OzakiStats* stats, int sms, cudaStream_t st) {
+  if (stats) {
+    // min_row, done_blocks and choice restart for every A (min_col belongs to B)
+    cudaError_t e = cudaMemsetAsync(&stats->min_row, 0xFF, sizeof(stats->min_row), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&stats->done_blocks, 0, sizeof(stats->done_blocks), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&stats->choice, 0xFF, sizeof(stats->choice), st);
+    if (e != cudaSuccess) return e;
+  }
+  switch (s) {
+    case 4: return prep_a_s<4>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 5: return prep_a_s<5>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 6: return prep_a_s<6>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 7: return prep_a_s<7>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 8: return prep_a_s<8>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 9: return prep_a_s<9>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_ozaki_decide(const unsigned long long* colsum, int n, int64_t k, OzakiStats* stats, int sms,
+                                cudaStream_t st) {
+  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 2));
+  ozaki_decide_kernel<<<blocks, 256, 0, st>>>(colsum, n, k, stats);
+  return cudaGetLastError();
 }
 
 }  // namespace cucosma

@@ -73,6 +73,15 @@ __device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
   }
 }
 
+// Fixed-point magnitudes of four values of a row (column) with exponent e:
+// sum_j floor(|v_j| 2^(30 - e)), each term below 2^30 since |v_j| < 2^e.
+__device__ __forceinline__ unsigned long long magnitude_fx4(const double (&v)[4], int e) {
+  unsigned long long t = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) t += __double2ull_rz(ldexp(fabs(v[j]), 30 - e));
+  return t;
+}
+
 // Packed slice layout shared by both operands: for row r (a row of A, or a
 // column of B), k-block kb = k / 32 and slice p, the 32 bytes of k-block kb
 // of slice p are at r * (kpad * S) + kb * (32 * S) + p * 32.  Four slices of

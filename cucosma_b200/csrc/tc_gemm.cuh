@@ -62,6 +62,12 @@ struct TcParams {
   // other per-problem fields above are ignored) and units = total_tiles.
   const GroupEntry* groups;
   int ngroups, total_tiles;
+  // Optional device-side gate: the kernel runs only if *gate == gate_value
+  // (the adaptive Ozaki call's slice count, chosen on the device).
+  const int* gate;
+  int gate_value;
+  // Ozaki: slices per k-block in the stacked B layout (0: the kernel's own count).
+  int b_layout_slices;
 };
 
 // Where a work unit's result goes (from TcParams, or from a GroupEntry).

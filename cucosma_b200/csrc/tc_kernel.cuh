@@ -157,16 +157,23 @@ __device__ __forceinline__ void issue_term(uint64_t ad0, uint64_t bd0, uint32_t 
   constexpr int KSTEPS = Tr::KSTEPS;
   constexpr int PA = Tr::kTerms.a[T], PB = Tr::kTerms.b[T], D = Tr::kTerms.d[T];
   constexpr bool FIRST = Tr::kTerms.first[T];
-  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, Tr::BN) : idesc_bf16_f32(128, Tr::BN);
+  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(Tr::TILE_M, Tr::BN) : idesc_bf16_f32(Tr::TILE_M, Tr::BN);
 #pragma unroll
   for (int kk = 0; kk < KSTEPS; ++kk) {
     const uint64_t ad = ad0 + (uint64_t)(Tr::a_off(PA, kk) >> 4);
     const uint64_t bd = bd0 + (uint64_t)(Tr::b_off(PB, kk) >> 4);
     const bool acc = (FIRST && kk == 0) ? not_first_kb : true;
-    if constexpr (Tr::kInt8)
-      mma_i8(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
-    else
-      mma_bf16(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+    if constexpr (Tr::kInt8) {
+      if constexpr (Tr::PAIR)
+        mma_i8_pair(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+      else
+        mma_i8(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+    } else {
+      if constexpr (Tr::PAIR)
+        mma_bf16_pair(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+      else
+        mma_bf16(acc0 + (uint32_t)(D * Tr::BN), ad, bd, IDESC, acc);
+    }
   }
 }
 template <class Tr, int... Ts>
@@ -198,14 +205,38 @@ __device__ __forceinline__ void issue_stacked(std::integer_sequence<int, Is...>,
   (issue_stacked_one<Tr, Is % Tr::NSUB, Is / Tr::NSUB>(ad0, b_base, acc0, not_first_kb), ...);
 }
 
+// Commit helpers: in a CTA pair the MMAs are issued by rank 0 for both CTAs
+// and their completion is signalled on the barrier at the same offset in
+// both CTAs (mask 0b11), or in rank 0 only (mask 0b01).
+template <bool PAIR>
+__device__ __forceinline__ void commit_both(uint64_t* bar) {
+  if constexpr (PAIR)
+    mma_commit_pair_mc(bar, 3);
+  else
+    mma_commit(bar);
+}
+template <bool PAIR>
+__device__ __forceinline__ void commit_self(uint64_t* bar) {
+  if constexpr (PAIR)
+    mma_commit_pair_mc(bar, 1);
+  else
+    mma_commit(bar);
+}
+
+// Register cap: what one CTA per SM can give each thread (see MAX_REGS).
 template <class Tr>
-__global__ void __launch_bounds__(Tr::THREADS, 1)
+__global__ void __maxnreg__(Tr::MAX_REGS)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
   constexpr int BN = Tr::BN, SWZ = Tr::SWZ, NA = Tr::NA, NB = Tr::NB, NACC = Tr::NACC, ST = Tr::STAGES;
   constexpr int A_REGION = Tr::A_REGION;
   constexpr int STAGE_BYTES = Tr::STAGE_BYTES;
   constexpr int NBUF = Tr::NBUF;
-  constexpr uint32_t IDESC = Tr::kInt8 ? idesc_s8_s32(128, BN) : idesc_bf16_f32(128, BN);
+  constexpr bool PAIR = Tr::PAIR;
+  constexpr int TILE_M = Tr::TILE_M;
+
+  // Not the path chosen on the device: every CTA (both of a pair) leaves
+  // before touching barriers or TMEM.
+  if (p.gate != nullptr && *p.gate != p.gate_value) return;
 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -222,6 +253,11 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.ngroups > 0 ? p.total_tiles : p.tiles_m * p.tiles_n * p.splits;
+  // CTA pair: rank 0 issues the MMAs of both CTAs; the pair (cluster) walks
+  // the units together.  Single CTA: rank 0, one CTA per unit.
+  const uint32_t rank = PAIR ? cluster_ctarank() : 0u;
+  const int unit0 = PAIR ? (int)cluster_id_x() : (int)blockIdx.x;
+  const int unit_step = PAIR ? (int)nclusters_x() : (int)gridDim.x;
   // K-blocks per accumulator chunk: with promotion the tensor cores
   // accumulate CHUNK k-blocks in TMEM and the epilogue warps add each chunk
   // into FP32 registers (round to nearest); otherwise one chunk per unit.
@@ -234,17 +270,25 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
     }
     for (int b = 0; b < 4; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], Tr::EPI_WARPS);
+      mbar_init(&tempty[b], Tr::EPI_WARPS * (PAIR ? 2 : 1));  // rank 0's: released by both CTAs' epilogues
     }
     mbar_init(drain, 1);
     fence_mbar_init();
   }
   if (warp == 1) {
-    tmem_alloc(tmem_holder, 512);
-    tmem_relinquish();
+    if constexpr (PAIR) {
+      tmem_alloc_pair(tmem_holder, 512);
+      tmem_relinquish_pair();
+    } else {
+      tmem_alloc(tmem_holder, 512);
+      tmem_relinquish();
+    }
   }
   tc_fence_before();
-  __syncthreads();
+  if constexpr (PAIR)
+    cluster_sync_all();  // both CTAs' barriers initialised before any remote arrive or load
+  else
+    __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_holder;
 
@@ -257,7 +301,7 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
       }
       int it = 0;  // global k-block counter (ring position)
       bool ok = true;
-      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+      for (int unit = unit0; unit < units && ok; unit += unit_step) {
         Unit u;
         resolve_unit(p, &tmA, &tmB, unit, u);
         const int tm = u.tm, tn = u.tn;
@@ -269,6 +313,14 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
           }
           uint8_t* st = stages + s * STAGE_BYTES;
           if (it == p.skip_stage) continue;  // test hook: this stage is never filled
+          if constexpr (PAIR) {
+            // Both CTAs' bytes complete on rank 0's full barrier; only rank 0 arrives.
+            if (rank == 0) mbar_arrive_expect_tx(&full[s], 2 * STAGE_BYTES);
+            const uint32_t bar0 = mapa_shared(smem_u32(&full[s]), 0);
+            tma_load_3d_pair(st, u.ta, kb * Tr::BK, tm * TILE_M + (int)rank * 128, 0, bar0);
+            tma_load_3d_pair(st + A_REGION, u.tb, kb * Tr::BK, tn * BN + (int)rank * Tr::BN_LOCAL, 0, bar0);
+            continue;
+          }
           mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
           if constexpr (Tr::PACKED) {
             // boxes of [rows][128 B]: slices 4j..4j+3 of k-block kb
@@ -276,9 +328,10 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
             for (int j = 0; j < Tr::TILES_A; ++j) tma_load_3d(st + j * Tr::A_TILE, u.ta, j * 128, kb, tm * 128, &full[s]);
             if constexpr (Tr::STACKED) {
               // per sub-tile one box [slices][SUB columns][32 B] of k-block kb
+              const int zs = p.b_layout_slices > 0 ? p.b_layout_slices : NB;  // slices per k-block in memory
 #pragma unroll
               for (int j = 0; j < Tr::NSUB; ++j)
-                tma_load_3d(st + A_REGION + j * Tr::B_SUB_BYTES, u.tb, 0, tn * BN + j * Tr::SUB, kb * NB, &full[s]);
+                tma_load_3d(st + A_REGION + j * Tr::B_SUB_BYTES, u.tb, 0, tn * BN + j * Tr::SUB, kb * zs, &full[s]);
             } else {
 #pragma unroll
               for (int j = 0; j < Tr::TILES_B; ++j)
@@ -291,22 +344,24 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
           }
         }
       }
-      if (!ok)  // drain loads that may still be in flight (bounded)
+      // Drain loads that may still be in flight (bounded).  In a pair, rank
+      // 0's full barriers count both CTAs' bytes.
+      if (!ok && rank == 0)
         for (int j = max(0, it - ST); j < it; ++j) mbar_wait(&full[j % ST], (j / ST) & 1, kErrTimeoutDrain, p.ctl);
     }
   } else if (warp == 1) {
     // -------------------------------------------------------- MMA issuer
-    if (lane == 0) {
+    if (lane == 0 && rank == 0) {
       int it = 0, ci = 0;
       bool ok = true;
-      for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+      for (int unit = unit0; unit < units && ok; unit += unit_step) {
         Unit u;
         resolve_unit(p, &tmA, &tmB, unit, u);
         const int kb1 = u.kb1;
         for (int cs = u.kb0; cs < kb1 && ok; cs += chunk, ++ci) {
           const int ce = min(kb1, cs + chunk);
           const int buf = ci % NBUF;
-          if (!mbar_wait(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+          if (!Tr::SPLIT && !mbar_wait(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
             ok = false;
             break;
           }
@@ -321,21 +376,37 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
             tc_fence_after();
             const uint32_t a_base = smem_u32(stages + s * STAGE_BYTES);
             const uint64_t ad0 = sdesc<SWZ>(a_base);
-            if constexpr (Tr::STACKED) {
+            if constexpr (Tr::SPLIT) {
+              // corrections (terms 0 .. NT-2, accumulator 1) once that
+              // accumulator is drained, then the main term (accumulator 0)
+              const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
+              if (kb == cs && !mbar_wait(&tempty[1], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT - 1>{}, ad0, bd0, acc0, kb != cs);
+              if (kb == cs && !mbar_wait(&tempty[0], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              issue_term<Tr, Tr::NT - 1>(ad0, bd0, acc0, kb != cs);
+            } else if constexpr (Tr::STACKED) {
               issue_stacked<Tr>(std::make_integer_sequence<int, Tr::NSUB * NA>{}, ad0, a_base + A_REGION, acc0,
                                 kb != cs);
             } else {
               const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
               issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT>{}, ad0, bd0, acc0, kb != cs);
             }
-            mma_commit(&empty[s]);  // stage free once these MMAs have read it
+            commit_both<PAIR>(&empty[s]);  // stage free (in both CTAs) once these MMAs have read it
           }
           if (!ok) break;
-          mma_commit(&tfull[buf]);  // accumulator ready once every MMA above completes
+          commit_both<PAIR>(&tfull[buf]);  // accumulator ready once every MMA above completes
         }
       }
       if (!ok) {
-        mma_commit(drain);  // wait (bounded) for every MMA issued so far
+        commit_self<PAIR>(drain);  // wait (bounded) for every MMA issued so far
         mbar_wait(drain, 0, kErrTimeoutDrain, p.ctl);
       }
     }
@@ -343,19 +414,31 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
     // ---------------------------------------------------------- epilogue
     // Epilogue warp ew: TMEM lane quadrant warp % 4 (the only lanes a warp may
     // access) and, with 8 epilogue warps, one half of the tile's columns.
+    // In a pair each CTA drains its own 128 rows of the 256-row tile.
     const int q = warp & 3;
     constexpr int W = Tr::COLS_PER_EW;
     const int colsub = ((warp - 2) / 4) * W;
     const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
     uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
+    // Releasing an accumulator: arrive on rank 0's tempty barrier idx.
+    auto release = [&](int idx) {
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if constexpr (PAIR)
+          mbar_arrive_cluster(mapa_shared(smem_u32(&tempty[idx]), 0));
+        else
+          mbar_arrive(&tempty[idx]);
+      }
+    };
     int ci = 0;
     bool ok = true;
-    for (int unit = blockIdx.x; unit < units && ok; unit += gridDim.x) {
+    for (int unit = unit0; unit < units && ok; unit += unit_step) {
       Unit u;
       resolve_unit(p, &tmA, &tmB, unit, u);
       const OutCtx o = out_ctx(p, u);
       const int z = u.z;
-      const int row0 = u.tm * 128 + 32 * q;
+      const int row0 = u.tm * TILE_M + (int)rank * 128 + 32 * q;
       const int col0 = u.tn * BN;
       prefetch_c_block(o, row0, col0 + (Tr::PROMOTE ? colsub : 0), Tr::PROMOTE ? W : BN, Tr::kInt8 ? 8 : 4, lane);
       if constexpr (Tr::PROMOTE) {
@@ -367,10 +450,16 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
           ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
           if (!ok) break;
           tc_fence_after();
-          Tr::accumulate(lane_base + (uint32_t)(buf * NACC * BN + colsub), master);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&tempty[buf]);
+          if constexpr (Tr::SPLIT) {
+            const uint32_t t = lane_base + (uint32_t)colsub;
+            Tr::accumulate_one(t, 1, master);  // corrections first: their MMAs resume first
+            release(1);
+            Tr::accumulate_one(t, 0, master);
+            release(0);
+          } else {
+            Tr::accumulate(lane_base + (uint32_t)(buf * NACC * BN + colsub), master);
+            release(buf);
+          }
         }
         if (!ok) break;
         Tr::finish(o, master, stg, lane, row0, col0 + colsub, z);
@@ -380,9 +469,7 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
         if (!ok) break;
         tc_fence_after();
         Tr::epilogue(o, lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
+        release(buf);
         ++ci;
       }
     }
@@ -390,10 +477,16 @@ __global__ void __launch_bounds__(Tr::THREADS, 1)
 
   tc_fence_before();
   __syncwarp();
-  __syncthreads();
+  if constexpr (PAIR)
+    cluster_sync_all();  // neither CTA leaves while the other may still signal its barriers
+  else
+    __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, 512);
+    if constexpr (PAIR)
+      tmem_dealloc_pair(tmem_base, 512);
+    else
+      tmem_dealloc(tmem_base, 512);
   }
 }
 
@@ -465,20 +558,33 @@ struct EpiF32 {
   // main product's accumulator 0 last) into the FP32 register accumulator,
   // rounding to nearest.
   // W columns of this warp (from tacc); accumulators STRIDE columns apart.
+  // With 128 register accumulators a thread loads 16 columns at a time (the
+  // loads of one chunk are off the MMA's critical path), otherwise 32.
   template <int W, int STRIDE, int NACC>
   static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[W]) {
 #pragma unroll
     for (int d = NACC - 1; d >= 0; --d) {
+      if constexpr (W > 64) {
 #pragma unroll
-      for (int c0 = 0; c0 < W; c0 += 32) {
-        uint32_t v0[16], v1[16];
-        tmem_ld16(tacc + d * STRIDE + c0, v0);
-        tmem_ld16(tacc + d * STRIDE + c0 + 16, v1);
-        tmem_ld_wait();
+        for (int c0 = 0; c0 < W; c0 += 16) {
+          uint32_t v0[16];
+          tmem_ld16(tacc + d * STRIDE + c0, v0);
+          tmem_ld_wait();
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          master[c0 + j] = __fadd_rn(master[c0 + j], __uint_as_float(v0[j]));
-          master[c0 + 16 + j] = __fadd_rn(master[c0 + 16 + j], __uint_as_float(v1[j]));
+          for (int j = 0; j < 16; ++j) master[c0 + j] = __fadd_rn(master[c0 + j], __uint_as_float(v0[j]));
+        }
+      } else {
+#pragma unroll
+        for (int c0 = 0; c0 < W; c0 += 32) {
+          uint32_t v0[16], v1[16];
+          tmem_ld16(tacc + d * STRIDE + c0, v0);
+          tmem_ld16(tacc + d * STRIDE + c0 + 16, v1);
+          tmem_ld_wait();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            master[c0 + j] = __fadd_rn(master[c0 + j], __uint_as_float(v0[j]));
+            master[c0 + 16 + j] = __fadd_rn(master[c0 + 16 + j], __uint_as_float(v1[j]));
+          }
         }
       }
     }
@@ -574,10 +680,16 @@ constexpr int kSmemBudget = 227 * 1024;
 // 128-byte swizzled row, so slice p sits in tile p / 4 at byte offset
 // (p % 4) * 32 -- selected like a K offset inside the swizzle atom.
 template <int NT_, int BN_, int SWZ_, int NA_, int NB_, int NACC_, bool INT8_, class Epi, bool PROMOTE_ = false,
-          int CHUNK_ = 0, int EPI_WARPS_ = 4, int SUB_ = 0>
+          int CHUNK_ = 0, int EPI_WARPS_ = 4, int SUB_ = 0, bool PAIR_ = false, bool SPLIT_ = false>
 struct TraitsBase {
   static constexpr int NT = NT_, BN = BN_, SWZ = SWZ_, NA = NA_, NB = NB_, NACC = NACC_;
   static constexpr bool kInt8 = INT8_;
+  // PAIR: a CTA pair (cluster of 2) computes a 256 x BN tile with
+  // cta_group::2 MMAs (M = 256); each CTA loads its 128 rows of A and BN / 2
+  // columns of B and holds its 128 rows x BN of the accumulator in its TMEM.
+  static constexpr bool PAIR = PAIR_;
+  static constexpr int TILE_M = PAIR_ ? 256 : 128;
+  static constexpr int BN_LOCAL = PAIR_ ? BN_ / 2 : BN_;
   // SUB > 0: stacked Ozaki form -- B slices of each SUB-column sub-tile
   // stacked along N (one [NB][SUB][32 B] box, 32-byte swizzle), NSUB
   // sub-tiles per tile, NACC = NB diagonal blocks per sub-tile.
@@ -587,10 +699,20 @@ struct TraitsBase {
   static constexpr int B_SUB_BYTES = STACKED ? NB_ * SUB_ * 32 : 0;
   static constexpr bool PROMOTE = PROMOTE_;
   static constexpr int CHUNK = CHUNK_;
+  // SPLIT: two promoted accumulators (corrections NACC-1 = 1, main 0) in one
+  // TMEM buffer, released separately: the epilogue drains the corrections
+  // first and frees them, so the next chunk's correction MMAs (issued first
+  // in every k-block) overlap the drain of the main accumulator.
+  static constexpr bool SPLIT = SPLIT_;
   // 4 epilogue warps (one per TMEM lane quadrant) or 8 (each quadrant
   // split into two column halves, so promoted register accumulators fit).
   static constexpr int EPI_WARPS = EPI_WARPS_;
   static constexpr int THREADS = (2 + EPI_WARPS) * 32;
+  // Registers a thread may hold: each of the SM's four sub-partitions has
+  // 16384 registers for the warps placed on it (ceil(warps / 4) of them).
+  static constexpr int WARPS_PER_SMSP = (THREADS / 32 + 3) / 4;
+  static constexpr int MAX_REGS = (16384 / (32 * WARPS_PER_SMSP)) / 8 * 8 > 255 ? 255
+                                                                               : (16384 / (32 * WARPS_PER_SMSP)) / 8 * 8;
   static constexpr int COLS_PER_EW = BN / (EPI_WARPS / 4);
   static_assert(EPI_WARPS == 4 || (EPI_WARPS == 8 && PROMOTE_), "8 epilogue warps only for promotion");
   static constexpr bool PACKED = INT8_;
@@ -598,7 +720,7 @@ struct TraitsBase {
   static constexpr int KSTEPS = PACKED ? 1 : SWZ / 32;
   static constexpr int TILES_A = PACKED ? (NA + 3) / 4 : NA;  // TMA boxes per operand per stage
   static constexpr int TILES_B = PACKED ? (NB + 3) / 4 : NB;
-  static constexpr int A_TILE = 128 * SWZ, B_TILE = BN * SWZ;
+  static constexpr int A_TILE = 128 * SWZ, B_TILE = BN_LOCAL * SWZ;
   static constexpr int A_REGION = TILES_A * A_TILE;
   static constexpr __host__ __device__ int a_off(int p, int kk) {
     return PACKED ? (p / 4) * A_TILE + (p % 4) * 32 : p * A_TILE + kk * 32;
@@ -614,6 +736,7 @@ struct TraitsBase {
   static_assert(!STACKED || (INT8_ && NSUB * SUB_ == BN_ && NB_ * SUB_ <= 256 && SUB_ % 16 == 0 &&
                              B_SUB_BYTES % 256 == 0 && NACC_ == NB_),
                 "stacked form: INT8, whole sub-tiles, MMA N <= 256");
+  static_assert(!PAIR_ || (!PACKED && BN_ % 32 == 0 && BN_ <= 256), "pair tiles: BF16 planes, MMA N <= 256");
   static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
   static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
   static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
@@ -621,13 +744,18 @@ struct TraitsBase {
   static_assert(STAGES >= 2, "at least a double-buffered ring");
   static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
   static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
-  static_assert(!PROMOTE || (CHUNK > 0 && NBUF >= 2), "promotion needs chunk buffers");
+  static_assert(!PROMOTE || (CHUNK > 0 && (NBUF >= 2 || SPLIT_)), "promotion needs chunk buffers");
+  static_assert(!SPLIT_ || (PROMOTE_ && NACC_ == 2 && NBUF == 1), "split release: two accumulators, one buffer");
   static __device__ __forceinline__ void epilogue(const OutCtx& p, uint32_t tacc, uint8_t* stg, int lane, int row0,
                                                   int col0, int z) {
     Epi::template run<BN>(p, tacc, stg, lane, row0, col0, z);
   }
   static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[COLS_PER_EW]) {
     if constexpr (PROMOTE) Epi::template accumulate<COLS_PER_EW, BN, NACC>(tacc, master);
+  }
+  // Accumulator d alone (split release).
+  static __device__ __forceinline__ void accumulate_one(uint32_t tacc, int d, float (&master)[COLS_PER_EW]) {
+    if constexpr (PROMOTE) Epi::template accumulate<COLS_PER_EW, BN, 1>(tacc + (uint32_t)(d * BN), master);
   }
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[COLS_PER_EW], uint8_t* stg,
                                                 int lane, int row0, int col0, int z) {
@@ -678,6 +806,26 @@ struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChu
       {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
+// CTA-pair tiles (256 rows): half the shared-memory operand reads and L2
+// traffic per output of the 128-row tiles at the same MMA N.
+//   Bf16x3Pair  256 x 256, one accumulator promoted every kPromoteChunk k-blocks.
+//   Bf16x6Pair  256 x 128, main and correction accumulators (as Bf16x6),
+//               double-buffered.
+//   Bf16x6PairWide 256 x 256, main and correction accumulators filling TMEM
+//               (one buffer, split release); the 256 x 128 tiles need about
+//               1.5x the L2-to-shared-memory bandwidth per flop.
+struct Bf16x3Pair : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8, 0, true> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
+};
+struct Bf16x6Pair : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true> {
+  static constexpr TermTable<6> kTerms{
+      {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
+};
+struct Bf16x6PairWide : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true, true> {
+  static constexpr TermTable<6> kTerms{
+      {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
+};
+
 // Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into
 // diagonal d = p + q.  Stacked form: S MMAs per sub-tile and k-block (one
 // per A slice, N shrinking with p) instead of S(S+1)/2 narrow ones -- an MMA
@@ -709,13 +857,67 @@ struct Ozaki : TraitsBase<S*(S + 1) / 2, OzakiBN<S>::value, 128, S, S, S, true, 
   static constexpr TermTable<S*(S + 1) / 2> kTerms = ozaki_terms<S>();
 };
 
+// Launch on `grid` CTAs (pair kernels: grid / 2 clusters of two CTAs; grid even).
 template <class Tr>
 static cudaError_t launch(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p, int grid, cudaStream_t st) {
   static std::atomic<uint64_t> attr_set{0};  // devices whose context has the limit raised
-  cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(tc_gemm_kernel<Tr>), Tr::SMEM, attr_set);
+  cudaError_t e = debug_cuda("smem attribute",
+                             ensure_smem_attr(reinterpret_cast<const void*>(tc_gemm_kernel<Tr>), Tr::SMEM, attr_set));
   if (e != cudaSuccess) return e;
+  if constexpr (Tr::PAIR) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(Tr::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = Tr::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    e = debug_cuda("pair kernel launch", cudaLaunchKernelEx(&cfg, tc_gemm_kernel<Tr>, a, b, p));
+    if (e != cudaSuccess) return e;
+    return debug_cuda("pair kernel launch (last error)", cudaGetLastError());
+  }
   tc_gemm_kernel<Tr><<<grid, Tr::THREADS, Tr::SMEM, st>>>(a, b, p);
-  return cudaGetLastError();
+  return debug_cuda("kernel launch", cudaGetLastError());
+}
+
+// Clusters of two CTAs of a pair kernel that can be resident at once on the
+// current device (one CTA per SM; a GPC with an odd SM count leaves one idle).
+template <class Tr>
+static int max_pair_clusters(int sms) {
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return sms / 2;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (v > 0) return v;
+  static std::atomic<uint64_t> attr_set{0};
+  if (ensure_smem_attr(reinterpret_cast<const void*>(tc_gemm_kernel<Tr>), Tr::SMEM, attr_set) != cudaSuccess)
+    return sms / 2;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(sms & ~1), 1, 1);
+  cfg.blockDim = dim3(Tr::THREADS, 1, 1);
+  cfg.dynamicSmemBytes = Tr::SMEM;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (debug_cuda("cluster occupancy",
+                 cudaOccupancyMaxActiveClusters(&n, reinterpret_cast<const void*>(tc_gemm_kernel<Tr>), &cfg)) !=
+          cudaSuccess ||
+      n <= 0) {
+    cudaGetLastError();
+    n = sms / 2;
+  }
+  cached[dev].store(n, std::memory_order_relaxed);
+  return n;
 }
 
 }  // namespace tc

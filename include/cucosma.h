@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CUCOSMA_VERSION 100 /* 0.1.0 */
+#define CUCOSMA_VERSION 200 /* 0.2.0 */
 
 #if defined(__GNUC__)
 #define CUCOSMA_API __attribute__((visibility("default")))
@@ -72,7 +72,8 @@ typedef struct cucosma_gemm_desc {
   int64_t lda, ldb, ldc;  /* row strides in elements */
   int32_t dtype;          /* cucosma_dtype (TYPE of config.h) */
   int32_t precision;      /* cucosma_precision */
-  int32_t slices;         /* Ozaki slice count 4..12, 0 = default (8) */
+  int32_t slices;         /* Ozaki slice count 4..9; 0 = chosen on the device per call: 8 or 9 slices,
+                           * or native FP64, from the operands' magnitude spread (see cucosma_plan_info) */
   int32_t epilogue;       /* cucosma_epilogue */
   double alpha, beta;     /* ALPHA, BETA of config.h; C is not read when beta == 0 */
   int32_t split_k;        /* SPLIT_K: 0 = library/tuner choice, >= 1 forced */
@@ -80,7 +81,10 @@ typedef struct cucosma_gemm_desc {
   int32_t tile;           /* 0 = library/tuner choice, else a kernel configuration id:
                            * NATIVE 1 = always the 128 x 128 tile kernel (no skinny-shape kernels),
                            *        2 = the 64 x 128 tile kernel (FP32; FP64 runs 128 x 128);
-                           * BF16X3 1 = 128 x 256 without promotion, 2 = 128 x 128 promoted */
+                           * BF16X3 1 = 128 x 256 without promotion, 2 = 128 x 128 promoted,
+                           *        3 = 128 x 256 promoted, 4 = 256 x 256 CTA pair (default when m > 128);
+                           * BF16X6 1 = 128 x 128, 2 = 256 x 128 CTA pair,
+                           *        3 = 256 x 256 CTA pair (default when m > 128) */
   int32_t flags;          /* 0, or CUCOSMA_FLAG_TEST_SKIP_STAGE */
 } cucosma_gemm_desc;
 
@@ -113,6 +117,14 @@ typedef struct cucosma_plan_info {
   int64_t kchunk;   /* K extent of one split */
   int64_t kpad;     /* padded K of the operand planes */
   uint64_t workspace_bytes, off_a, off_b, off_ea, off_eb, off_part;
+  /* Ozaki with slices = 0 (the default): the slice count is chosen on the
+   * device from the operands (8 or 9 slices, or native FP64 when 9 cannot
+   * reach FP64 accuracy; see cucosma_gemm_desc.slices).  The call writes its
+   * choice as an int32 at workspace offset off_choice: 8, 9, or 0 = native
+   * FP64.  0 for every other path. */
+  uint64_t off_choice;
+  int32_t layout_slices; /* Ozaki: slices per 32-wide k-block in the workspace layout */
+  int32_t reserved;
 } cucosma_plan_info;
 CUCOSMA_API cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cucosma_plan_info* info);
 
@@ -123,13 +135,27 @@ CUCOSMA_API cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cuc
 CUCOSMA_API cucosma_status cucosma_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* cucosma_gemm with a library-managed workspace (the same per-device,
+ * per-stream buffer as cucosma_sgemm below, with the same rules on stream
+ * capture) instead of a caller-owned one: the reference's split-K path
+ * allocated its workspace inside the call (cuCOSMAV100.cuh:2828-2838); this
+ * keeps that interface for every precision without allocating per call.
+ * Used by the C++ drop-in (cucosma.hpp). */
+CUCOSMA_API cucosma_status cucosma_gemm_managed(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
+                                                void* stream);
+
 /* Reference-shaped FP32 / FP64 entry points: the compile-time M, N, K, ALPHA,
  * BETA of config.h become arguments (cuCOSMAV100.cuh:2774; the FP64 form is
  * the TYPE=double instantiation).  Native arithmetic, no epilogue; any split-K
- * workspace is library-managed (allocated once per device and stream and
- * grown on demand, like the reference's internal cudaMalloc but not per
- * call), so the first split-K call on a stream must not be inside a stream
- * capture. */
+ * workspace is library-managed (one buffer per device and stream, allocated
+ * and grown on demand, like the reference's internal cudaMalloc but not per
+ * call).  Growing it synchronises the stream and frees the old buffer, so any
+ * call that needs a larger workspace than the stream's buffer holds must not
+ * be inside a stream capture: during a capture such a call returns
+ * CUCOSMA_STATUS_ALLOC_FAILED instead of allocating.  The buffer is keyed by
+ * the stream handle and kept until the process exits; a stream that is
+ * destroyed while work on it still uses the buffer must not have its handle
+ * reused by a new stream before that work completes. */
 CUCOSMA_API cucosma_status cucosma_sgemm(int m, int n, int k, float alpha, const float* A, int lda, const float* B, int ldb,
                              float beta, float* C, int ldc, void* stream);
 CUCOSMA_API cucosma_status cucosma_dgemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb,

@@ -46,8 +46,9 @@ inline cublasStatus_t to_cublas(cucosma_status s) {
 }
 
 // Full form: precision (cucosma_precision) and epilogue (cucosma_epilogue)
-// selectable; the split-K workspace is library-managed like the reference's
-// (allocated once per device and grown on demand instead of per call).
+// selectable; the workspace is library-managed like the reference's split-K
+// buffer (one per device and stream, grown on demand instead of allocated
+// and freed per call: cucosma_gemm_managed).
 template <int kM, int kN, int kK, class T>
 cublasStatus_t cosmaGemm(const T* A, int lda, const T* B, int ldb, T* C, int ldc, T alpha, T beta,
                          int precision, int epilogue, cudaStream_t stream) {
@@ -73,17 +74,7 @@ cublasStatus_t cosmaGemm(const T* A, int lda, const T* B, int ldb, T* C, int ldc
     return to_cublas(cucosma_dgemm(kM, kN, kK, (double)alpha, (const double*)A, lda, (const double*)B, ldb,
                                    (double)beta, (double*)C, ldc, stream));
   }
-  size_t need = 0;
-  cucosma_status s = cucosma_gemm_workspace_size(&d, &need);
-  if (s != CUCOSMA_STATUS_SUCCESS) return to_cublas(s);
-  void* ws = nullptr;
-  if (need && cudaMalloc(&ws, need) != cudaSuccess) return CUBLAS_STATUS_ALLOC_FAILED;
-  s = cucosma_gemm(&d, A, B, C, ws, need, stream);
-  if (ws) {
-    cudaStreamSynchronize(stream);
-    cudaFree(ws);
-  }
-  return to_cublas(s);
+  return to_cublas(cucosma_gemm_managed(&d, A, B, C, stream));
 }
 
 }  // namespace cucosma

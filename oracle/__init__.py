@@ -130,6 +130,37 @@ def ozaki_slices(A, B, s):
     return ea, eb, sa, sb
 
 
+def ozaki_magnitude_sums(A, B):
+    """Fixed-point magnitude sums of the adaptive Ozaki path: per row i of A,
+    sum_k floor(|a_ik| 2^(30 - ea_i)); per column j of B the same with eb_j
+    (ea, eb the Ozaki exponents).  Exact integers (Python ints)."""
+    A, B = _f64(A), _f64(B)
+    ea, eb = ozaki_exponents(A, B)
+    ra = np.floor(np.ldexp(np.abs(A), (30 - ea.astype(np.int64))[:, None])).astype(np.uint64)
+    rb = np.floor(np.ldexp(np.abs(B), (30 - eb.astype(np.int64))[None, :])).astype(np.uint64)
+    return [int(x) for x in ra.sum(axis=1, dtype=np.uint64)], [int(x) for x in rb.sum(axis=0, dtype=np.uint64)]
+
+
+def ozaki_choice(A, B):
+    """Restatement of the device's path choice for the default Ozaki call
+    (ozaki_choice in cucosma_b200/csrc/split.cuh): with P = K 2^30 / min
+    nonzero row sum and Q = K 2^30 / min nonzero column sum, the smallest s in
+    {8, 9} with 7 s >= 53 + log2(P + Q), else 0 (native FP64); 8 when A or B
+    is all zero."""
+    k = np.asarray(A).shape[1]
+    sa, sb = ozaki_magnitude_sums(A, B)
+    nza, nzb = [x for x in sa if x], [x for x in sb if x]
+    if not nza or not nzb:
+        return 8
+    P = k * 1073741824.0 / float(min(nza))
+    Q = k * 1073741824.0 / float(min(nzb))
+    need = 53.0 + np.log2(P + Q)
+    for s in (8, 9):
+        if 7.0 * s >= need:
+            return s
+    return 0
+
+
 def ozaki_gemm(A, B, s, Cin=None, alpha=1.0, beta=0.0, epilogue=EPI_NONE, kchunk=0, threads=0):
     """Bit-exact restatement of the Ozaki INT8-slice DGEMM (see oracle.c)."""
     A, B = _f64(A), _f64(B)

@@ -159,3 +159,47 @@ def test_backward_rejects_bad_arguments():
     assert st == cc.MISALIGNED
     st = L.cucosma_gemm_backward(C.byref(d), f, f, f, 64, None, 64, f, 64, None, 0, f, n.value, None)
     assert st == cc.INVALID_VALUE
+
+
+def test_backward_with_tuned_subproblem_fits_queried_workspace(tmp_path):
+    """A tuning-cache entry for the dB product (k x n x m, BF16x3) that forces
+    one split: the queried workspace then has no split-K partials region, and
+    the backward call must run the product with that same tuned plan.  A
+    guard band after the queried workspace must stay untouched and the
+    gradients must still match FP64."""
+    import ctypes as C
+
+    import torch
+
+    m, n, k = 4096, 512, 512
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    cache = tmp_path / "tune.txt"
+    # v1 <sms> <dtype> <precision> <slices> <m> <n> <k> <split_k> <swizzle> <tile> <ms>: the dB product
+    cache.write_text("v1 %d 0 1 0 %d %d %d 1 0 0 1.0\n" % (sms, k, n, m))
+    cc.tune_cache_clear()
+    try:
+        cc.tune_cache_load(str(cache))
+        A = uniform(14, (m, k), lo=-0.1, hi=0.1)
+        B = uniform(15, (k, n), lo=-0.1, hi=0.1)
+        W = uniform(16, (m, n))
+        dA_, dB_, dY = to_dev(A), to_dev(B), to_dev(W)
+        Y = to_dev(np.zeros((m, n), np.float32))
+        cc.gemm(dA_, dB_, Y, 1.0, 0.0, precision="bf16x3", epilogue="sigmoid")
+        d = cc.make_desc(dA_, dB_, Y, 1.0, 0.0, precision="bf16x3", epilogue="sigmoid")
+        need = C.c_size_t(0)
+        assert cc.lib().cucosma_gemm_backward_workspace_size(C.byref(d), C.byref(need)) == cc.SUCCESS
+        guard = 1 << 20
+        buf = torch.full((need.value + guard,), 0x5A, dtype=torch.uint8, device="cuda")
+        gA = to_dev(np.zeros((m, k), np.float32))
+        gB = to_dev(np.zeros((k, n), np.float32))
+        cc.gemm_backward(dA_, dB_, Y, dY, gA, gB, precision="bf16x3", epilogue="sigmoid",
+                         workspace=buf[: need.value])
+        torch.cuda.synchronize()
+        assert bool((buf[need.value:] == 0x5A).all()), "backward wrote past the queried workspace"
+        Yh = Y.cpu().numpy().astype(np.float64)
+        G = W.astype(np.float64) * Yh * (1 - Yh)
+        refA, refB = oracle.gemm(G, B.T.astype(np.float64)), oracle.gemm(A.T.astype(np.float64), G)
+        assert np.abs(gA.cpu().numpy() - refA).max() <= 2e-4 * np.abs(refA).max()
+        assert np.abs(gB.cpu().numpy() - refB).max() <= 2e-4 * np.abs(refB).max()
+    finally:
+        cc.tune_cache_clear()

@@ -43,7 +43,7 @@ def run(A, B, Cin, alpha, beta, precision, epilogue="none", slices=0, split_k=0,
 
 
 SHAPES = [(1, 1, 1), (7, 5, 3), (128, 256, 32), (129, 257, 33), (300, 200, 100), (256, 512, 1024), (1000, 64, 77),
-          (64, 1000, 2000)]
+          (64, 1000, 2000), (513, 300, 700), (600, 520, 3000)]
 
 
 @pytest.mark.parametrize("precision,nterms", [("bf16x3", 2), ("bf16x6", 3)])
@@ -61,8 +61,13 @@ def test_split_planes_bitexact(precision, nterms):
     assert np.array_equal(pb, oracle.split_bf16(np.ascontiguousarray(B.T), nterms))
 
 
-@pytest.mark.parametrize("precision,nterms,tile", [("bf16x3", 2, 0), ("bf16x3", 2, 2), ("bf16x6", 3, 0)],
-                         ids=["bf16x3", "bf16x3promoted", "bf16x6"])
+BF16_VARIANTS = [("bf16x3", 2, 0), ("bf16x3", 2, 1), ("bf16x3", 2, 2), ("bf16x3", 2, 3), ("bf16x6", 3, 0),
+                 ("bf16x6", 3, 1), ("bf16x6", 3, 2)]
+
+
+@pytest.mark.parametrize("precision,nterms,tile", BF16_VARIANTS,
+                         ids=["bf16x3-pair256x256", "bf16x3-128x256wide", "bf16x3-128x128", "bf16x3-128x256",
+                              "bf16x6-pair256x256", "bf16x6-128x128", "bf16x6-pair256x128"])
 @pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d" % s for s in SHAPES])
 def test_bf16_paths_vs_oracle(precision, nterms, tile, shape):
     m, n, k = shape
@@ -261,3 +266,95 @@ def test_ozaki_zero_rows_and_columns():
     assert np.array_equal(ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32), ea)
     assert np.array_equal(ws[plan["off_eb"]: plan["off_eb"] + 4 * n].view(np.int32), eb)
     assert np.array_equal(out, oracle.ozaki_gemm(A, B, s))
+
+
+# ------------------------------------------- FP32 accuracy bar, adaptive Ozaki
+
+
+@pytest.mark.parametrize("dist", ["uniform", "spread"])
+def test_default_bf16x6_not_worse_than_native_fp32_at_k8192(dist):
+    """The FP32-accurate tensor-core form (BF16x6 with its default CTA-pair
+    tile) is at least as accurate as the native FP32 kernel -- whose FFMA
+    accumulation follows the reference kernel's inner loop
+    (cuCOSMAV100.cuh:657-675) -- normwise and in mean relative error, on
+    1024 x 1024 x 8192 with uniform[-1, 1] entries and with entries
+    sign * exp(N(0, 8^2)); errors on 64 sampled rows against the FP64 oracle."""
+    m, n, k = 1024, 1024, 8192
+    if dist == "uniform":
+        A, B = uniform(50, (m, k)), uniform(51, (k, n))
+    else:
+        A, B = expspread(50, (m, k), dtype=np.float32), expspread(51, (k, n), dtype=np.float32)
+    Cin = np.zeros((m, n), np.float32)
+    rows = np.linspace(0, m - 1, 64).astype(np.int64)
+    ref = oracle.gemm(A[rows], B)
+    out6, plan6 = run(A, B, Cin, 1.0, 0.0, "bf16x6")
+    outn, _ = run(A, B, Cin, 1.0, 0.0, "native")
+    e6, en = oracle.errors(out6[rows], ref), oracle.errors(outn[rows], ref)
+    print(dist, "bf16x6", plan6["tile_m"], plan6["tile_n"], e6, "native", en)
+    assert plan6["tile_m"] == 256  # the CTA-pair tile is the default
+    assert e6["normwise"] <= en["normwise"]
+    assert e6["mean_rel"] <= en["mean_rel"]
+
+
+def _choice(ws, plan):
+    return int(ws[plan["off_choice"]: plan["off_choice"] + 4].view(np.int32)[0])
+
+
+def test_ozaki_default_uniform_chooses_8_slices_bitexact():
+    """Default descriptor (slices = 0) on uniform entries: the device picks
+    8 slices, and the result is bit-exact against the restatement with 8
+    slices (the 9-slice workspace layout holds the 8-slice decomposition in
+    its first 8 slices)."""
+    m = n = k = 1024
+    A, B = uniform(60, (m, k), np.float64), uniform(61, (k, n), np.float64)
+    Cin = uniform(62, (m, n), np.float64)
+    out, plan, ws = run(A, B, Cin, 1.0, 0.5, "ozaki", keep_ws=True)
+    assert plan["slices"] == 0 and plan["layout_slices"] == 9
+    assert _choice(ws, plan) == 8 == oracle.ozaki_choice(A, B)
+    kchunk = plan["kchunk"] if plan["splits"] > 1 else 0
+    assert np.array_equal(out, oracle.ozaki_gemm(A, B, 8, Cin=Cin, alpha=1.0, beta=0.5, kchunk=kchunk))
+
+
+def test_ozaki_default_spread_falls_back_to_native_fp64():
+    """Default descriptor on entries sign * exp(N(0, 8^2)): nine slices
+    cannot reach FP64 accuracy, so the call runs native FP64; the result is
+    the native kernel's bit for bit, and normwise <= max(1e-15, native's)
+    against the double-double oracle."""
+    m = n = k = 1024
+    A, B = expspread(63, (m, k)), expspread(64, (k, n))
+    Cin = np.zeros((m, n))
+    out, plan, ws = run(A, B, Cin, 1.0, 0.0, "ozaki", keep_ws=True)
+    assert _choice(ws, plan) == 0
+    nat, _ = run(A, B, Cin, 1.0, 0.0, "native", tile=1)
+    assert np.array_equal(out, nat)
+    hi, lo = oracle.gemm(A, B, dd=True)
+    eo, en = oracle.errors(out, hi, lo), oracle.errors(nat, hi, lo)
+    print("spread: ozaki default", eo, "native", en)
+    assert eo["normwise"] <= max(1e-15, en["normwise"])
+
+
+def test_ozaki_default_moderate_spread_chooses_9_slices_bitexact():
+    """Entries sign * exp(N(0, 1)): the device picks 9 slices; bit-exact
+    against the 9-slice restatement and within 1e-15 normwise of the
+    double-double oracle."""
+    m = n = k = 768
+    A, B = expspread(65, (m, k), sigma=1.0), expspread(66, (k, n), sigma=1.0)
+    Cin = np.zeros((m, n))
+    out, plan, ws = run(A, B, Cin, 1.0, 0.0, "ozaki", keep_ws=True)
+    assert _choice(ws, plan) == 9
+    assert np.array_equal(out, oracle.ozaki_gemm(A, B, 9))
+    hi, lo = oracle.gemm(A, B, dd=True)
+    assert oracle.errors(out, hi, lo)["normwise"] <= 1e-15
+
+
+def test_ozaki_choice_matches_host_restatement():
+    """The device's path choice equals the oracle's restatement computed from
+    the same fixed-point row and column magnitude sums."""
+    for seed, sigma in ((70, 0.0), (71, 1.0), (72, 2.0), (73, 4.0)):
+        m, n, k = 200, 150, 300
+        if sigma == 0.0:
+            A, B = uniform(seed, (m, k), np.float64), uniform(seed + 100, (k, n), np.float64)
+        else:
+            A, B = expspread(seed, (m, k), sigma=sigma), expspread(seed + 100, (k, n), sigma=sigma)
+        _, plan, ws = run(A, B, np.zeros((m, n)), 1.0, 0.0, "ozaki", keep_ws=True)
+        assert _choice(ws, plan) == oracle.ozaki_choice(A, B), (seed, sigma)
