@@ -3,16 +3,28 @@
 Workload (single GPU): the precision forms at M = N = K = 8192, alpha = 1,
 beta = 0, entries i.i.d. uniform[-1, 1] from fixed seeds (synthetic; the
 reference uses no dataset).  The headline "step" is one FP32 SGEMM through
-the BF16x3 tensor-core path (split pre-pass + tcgen05 GEMM); the same
-protocol times the native FP32 (FFMA2) SGEMM, the native FP64 (FP64 tensor-core MMA)
-DGEMM and the Ozaki INT8-slice DGEMM, each reported with TFLOP/s, % of its
-relevant peak and its error against an FP64 (double-double for FP64 paths)
-CPU oracle evaluated on a sample of rows.
+the FP32-accurate BF16x6 tensor-core path (split pre-pass + CTA-pair tcgen05
+GEMM), whose error against FP64 is at or below the native FP32 kernel's; the
+same protocol times BF16x3 (faster, less accurate), the native FP32 (FFMA2)
+SGEMM, the native FP64 (FP64 tensor-core MMA) DGEMM and the Ozaki INT8-slice
+DGEMM (default call: 8 or 9 slices or native FP64, chosen on the device),
+each reported with TFLOP/s, % of its relevant peak and its error against an
+FP64 (double-double for FP64 paths) CPU oracle evaluated on a sample of rows.
+results.spread repeats the forms on exponent-spread entries
+sign * exp(N(0, 8^2)); results.families runs the reference's shape families
+(square 8192^3, flat 16384^2 x 256, large-K 256^2 x 1,048,576, large-N
+256 x 1,048,576 x 256) at alpha = 1, beta = 0.5, with and without the fused
+sigmoid, through every path, with compute- and HBM-roofline fractions.
 
 Timing: W untimed warm-up steps, then exactly K steps bracketed by a
 barrier and torch.cuda.synchronize(), CUDA events on the launching stream,
 max over ranks.  Every input is larger than the 126 MB L2 (256 MB per FP32
 operand), so no flush is needed between steps.
+
+cpu_baseline: the FP64 oracle (the reference's CPU product order,
+Matrix.h:183-201) on a bounded sample of rows of the 8192^3 workload on all
+host threads, plus the whole 1024^3 plain configuration single-threaded and
+on all threads (cpu_baseline.p1024).
 
 --impl reference times the reference's own CPU product
 (Matrix<double>::operator*, Kernel/cuda/src/Matrix.h:183-201, built from its
@@ -44,7 +56,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "TFLOP/s & % of peak: BF16x3/Ozaki vs native S/DGEMM at stated error vs FP64"
-OZAKI_SLICES = 8
+OZAKI_SLICES = 0  # the default call: 8 or 9 slices or native FP64, chosen on the device
 
 
 def dram_traffic(path, n):
@@ -418,6 +430,181 @@ def cpu_sample(n, A32, B32, A64, B64, outs, budget_s=12.0):
     return cpu, errs
 
 
+FAMILIES = [("SQ", 8192, 8192, 8192), ("FL", 16384, 16384, 256), ("LK", 256, 256, 1048576),
+            ("LN", 256, 1048576, 256)]
+FAMILY_PATHS = [("native_f32", "native", 4), ("bf16x3", "bf16x3", 4), ("bf16x6", "bf16x6", 4),
+                ("native_f64", "native", 8), ("ozaki", "ozaki", 8)]
+
+
+def families_bench(cc, pk, sms, steps, warmup, check_rows=4):
+    """The reference's benchmark shape families (Benchmarks/TESTS_TO_RUN
+    square / Flat / LargeK / LargeN) at the sizes the workload names, alpha = 1,
+    beta = 0.5 with C uniform[-1, 1], without and with the fused sigmoid,
+    through every path (Ozaki with its default, device-chosen slice count).
+    Per entry: GPU time of one call (CUDA events over `steps` calls after
+    `warmup`; every operand or C is larger than L2 except FL's 16 MB A and B),
+    TFLOP/s, the fraction of the path's compute peak, the fraction of the
+    HBM roofline for the algorithmic bytes sizeof(T) (MK + KN + 2MN), and the
+    error on `check_rows` sampled rows of the first call's output against the
+    FP64 oracle (FP32 paths) or the double-double oracle (FP64 paths)."""
+    import torch
+
+    import oracle
+
+    out = {}
+    hbm = pk["hbm"] * 1e9
+    for fam, m, n, k in FAMILIES:
+        flop = 2.0 * m * n * k
+        for dt in (torch.float32, torch.float64):
+            es = 4 if dt == torch.float32 else 8
+            A = make_rect(m, k, 100, dt)
+            B = make_rect(k, n, 101, dt)
+            C0 = make_rect(m, n, 102, dt)
+            rows = np.linspace(0, m - 1, check_rows).astype(np.int64)
+            An, Bn, C0n = A[rows].double().cpu().numpy(), B.double().cpu().numpy(), C0[rows].double().cpu().numpy()
+            refs = {}
+            for name, prec, pes in FAMILY_PATHS:
+                if pes != es:
+                    continue
+                for epi in ("none", "sigmoid"):
+                    Cm = C0.clone()
+                    d = cc.make_desc(A, B, Cm, 1.0, 0.5, precision=prec, epilogue=epi)
+                    ws = cc.alloc_workspace(d)
+                    plan = cc.get_plan(d)
+                    cc.gemm(A, B, Cm, 1.0, 0.5, precision=prec, epilogue=epi, workspace=ws)
+                    torch.cuda.synchronize()
+                    first = Cm[rows].double().cpu().numpy()
+                    choice = None
+                    if prec == "ozaki" and plan["off_choice"]:
+                        choice = int(ws[plan["off_choice"]: plan["off_choice"] + 4].view(torch.int32).item())
+                    for _ in range(warmup):
+                        cc.gemm(A, B, Cm, 1.0, 0.5, precision=prec, epilogue=epi, workspace=ws)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(steps):
+                        cc.gemm(A, B, Cm, 1.0, 0.5, precision=prec, epilogue=epi, workspace=ws)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    ms = e0.elapsed_time(e1) / steps
+                    if epi not in refs:
+                        code = oracle.EPI_SIGMOID if epi == "sigmoid" else oracle.EPI_NONE
+                        refs[epi] = oracle.gemm(An, Bn, C0n, 1.0, 0.5, code, dd=(es == 8))
+                    ref = refs[epi]
+                    err = oracle.errors(first, *ref) if es == 8 else oracle.errors(first, ref)
+                    peak = path_peak(name, pk, sms, choice if choice else 8)
+                    algo = es * (m * k + k * n + 2 * m * n)
+                    tf = flop / (ms * 1e-3) / 1e12
+                    e = {"ms": ms, "tflops": tf, "compute_frac": tf / peak, "hbm_frac": algo / (ms * 1e-3) / hbm,
+                         "algorithmic_bytes": algo, "normwise": err["normwise"], "max_abs": err["max_abs"],
+                         "tile": [plan["tile_m"], plan["tile_n"]], "splits": plan["splits"]}
+                    if choice is not None:
+                        e["ozaki_choice"] = choice
+                    out["%s_%s_%s" % (fam, name, epi)] = e
+                    del ws, Cm
+            del A, B, C0
+            torch.cuda.empty_cache()
+    out["inputs"] = "uniform[-1, 1], seeds 100 / 101 / 102 (A / B / C), alpha = 1, beta = 0.5"
+    return out
+
+
+def spread_bench(cc, n, pk, sms, steps, warmup, no_cpu=False, check_rows=4):
+    """The precision forms on exponent-spread entries sign * exp(X), X ~ N(0,
+    sigma = 8) at n^3 (alpha = 1, beta = 0): FP32 paths on the FP32 rounding
+    of the FP64 values, FP64 paths on the values themselves (the default
+    Ozaki call chooses its path on the device: reported as ozaki_choice).
+    Time per call (CUDA events) and the error on sampled rows against the
+    FP64 / double-double oracle."""
+    import torch
+
+    import oracle
+
+    A64 = make_dist(n, 11, "spread")
+    B64 = make_dist(n, 12, "spread")
+    rows = np.linspace(0, n - 1, check_rows).astype(np.int64)
+    flop = 2.0 * n ** 3
+    res = {}
+    ref = None
+    for dt, names in ((torch.float32, ("native_f32", "bf16x3", "bf16x6")), (torch.float64, ("native_f64", "ozaki"))):
+        A, B = (A64.float(), B64.float()) if dt == torch.float32 else (A64, B64)
+        if not no_cpu:
+            ref = oracle.gemm(A[rows].double().cpu().numpy(), B.double().cpu().numpy(), dd=(dt == torch.float64))
+        for name in names:
+            prec = "native" if name.startswith("native") else name
+            Cm = torch.zeros((n, n), device="cuda", dtype=dt)
+            d = cc.make_desc(A, B, Cm, precision=prec)
+            ws = cc.alloc_workspace(d)
+            plan = cc.get_plan(d)
+            cc.gemm(A, B, Cm, precision=prec, workspace=ws)
+            for _ in range(warmup):
+                cc.gemm(A, B, Cm, precision=prec, workspace=ws)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                cc.gemm(A, B, Cm, precision=prec, workspace=ws)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            e = {"ms": ms, "tflops": flop / (ms * 1e-3) / 1e12}
+            if name == "ozaki" and plan["off_choice"]:
+                e["ozaki_choice"] = int(ws[plan["off_choice"]: plan["off_choice"] + 4].view(torch.int32).item())
+            if ref is not None:
+                o = Cm[rows].double().cpu().numpy()
+                er = oracle.errors(o, *ref) if dt == torch.float64 else oracle.errors(o, ref)
+                e["normwise"], e["mean_rel"] = er["normwise"], er["mean_rel"]
+            res[name] = e
+            del ws, Cm
+        del A, B
+    res["inputs"] = "sign * exp(N(0, 8^2)) per entry, %d^3, seeds 11 / 12" % n
+    return res
+
+
+def make_rect(rows, cols, seed, dtype):
+    import torch
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    return torch.rand((rows, cols), generator=g, device="cuda", dtype=dtype) * 2 - 1
+
+
+def path_peak(name, pk, sms, slices):
+    """Compute peak (TFLOP/s of useful flops) of a path."""
+    if name == "native_f32":
+        return sms * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12
+    if name == "native_f64":
+        return sms * 64 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12
+    if name == "bf16x3":
+        return pk["bf16"] / 3
+    if name == "bf16x6":
+        return pk["bf16"] / 6
+    return 2 * pk["bf16"] / (slices * (slices + 1) / 2)
+
+
+def cpu_1024():
+    """The reference-order FP64 product (Matrix.h:183-201, the oracle's
+    restatement) on the whole 1024^3 problem of the plain configuration,
+    single-threaded and on every host thread."""
+    import oracle
+
+    rng = np.random.default_rng(1)
+    A = rng.uniform(-1, 1, (1024, 1024))
+    B = rng.uniform(-1, 1, (1024, 1024))
+    res = {}
+    for label, th in (("single_thread", 1), ("all_threads", oracle.lib().oracle_max_threads())):
+        t0 = time.perf_counter()
+        oracle.gemm(A, B, threads=th)
+        dt = time.perf_counter() - t0
+        res[label] = {"threads": th, "s": dt, "tflops": 2.0 * 1024 ** 3 / dt / 1e12}
+    try:
+        model = [ln.split(":", 1)[1].strip() for ln in open("/proc/cpuinfo") if ln.startswith("model name")][0]
+    except Exception:
+        model = None
+    res["cpu"] = model
+    res["nproc"] = os.cpu_count()
+    return res
+
+
 def reference_arm(args):
     """--impl reference: the reference's own CPU product on host threads."""
     import ctypes as C
@@ -533,6 +720,8 @@ def main():
                     "bf16x3,bf16x6,native_f32,ozaki,native_f64,grouped_bf16x3,grouped_ozaki,fwd_bwd")
     ap.add_argument("--precision-sweep", action="store_true", help="precision forms x sizes x distributions")
     ap.add_argument("--sweep-sizes", default="8192,16384")
+    ap.add_argument("--no-families", action="store_true", help="skip the reference shape families")
+    ap.add_argument("--family-steps", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -568,6 +757,8 @@ def main():
     # region alone is tens of milliseconds, shorter than the sampling period).
     sampler = ClockSampler(local)
     sampler.start()
+    peak_names = {"native_f32": "FP32 SIMT (SMs x 128 x 2 x max clock)", "native_f64": "FP64 (SMs x 64 x 2 x max clock)",
+                  "bf16x3": "measured bf16 dense / 3 products", "bf16x6": "measured bf16 dense / 6 products"}
     for name, A, B, Cm, slices in paths:
         prec = "native" if name.startswith("native") else name
         d = cc.make_desc(A, B, Cm, 1.0, 0.0, precision=prec, slices=slices)
@@ -579,23 +770,29 @@ def main():
                 results[name] = {"available": False}
                 continue
             raise
+        plan = cc.get_plan(d)
+        choice = None
+        if name == "ozaki":
+            torch.cuda.synchronize()
+            choice = (int(ws[plan["off_choice"]: plan["off_choice"] + 4].view(torch.int32).item())
+                      if plan["off_choice"] else slices)
         ms, kern_ms, launches = time_path(cc, A, B, Cm, prec, slices, args.steps, args.warmup, world, ws)
         ms = max_over_ranks(ms, world)
         tf = flop / (ms * 1e-3) / 1e12
-        if name == "native_f32":
-            peak, peak_name = sms * 128 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12, "FP32 SIMT (SMs x 128 x 2 x max clock)"
-        elif name == "native_f64":
-            peak, peak_name = sms * 64 * 2 * pk["sm_max_mhz"] * 1e6 / 1e12, "FP64 (SMs x 64 x 2 x max clock)"
-        elif name == "bf16x3":
-            peak, peak_name = pk["bf16"] / 3, "measured bf16 dense / 3 products"
-        elif name == "bf16x6":
-            peak, peak_name = pk["bf16"] / 6, "measured bf16 dense / 6 products"
+        if name == "ozaki":
+            sl = choice if choice else 8
+            peak = path_peak(name, pk, sms, sl)
+            peak_name = "INT8 dense (2 x measured bf16) / %d slice products" % (sl * (sl + 1) // 2)
         else:
-            peak = 2 * pk["bf16"] / (slices * (slices + 1) / 2)
-            peak_name = "INT8 dense (2 x measured bf16) / %d slice products" % (slices * (slices + 1) // 2)
+            peak, peak_name = path_peak(name, pk, sms, 0), peak_names[name]
         results[name] = {"available": True, "ms": ms, "tflops": tf, "pct_of_peak": 100.0 * tf / peak,
                          "peak_tflops": peak, "peak": peak_name, "kernel_ms": kern_ms, "launches_per_step":
-                         launches / args.steps, "workspace_bytes": (ws.numel() if ws is not None else 0)}
+                         launches / args.steps, "workspace_bytes": (ws.numel() if ws is not None else 0),
+                         "tile": [plan["tile_m"], plan["tile_n"]]}
+        if kern_ms:
+            results[name]["kernel_frac"] = flop / (kern_ms * 1e-3) / 1e12 / peak
+        if choice is not None:
+            results[name]["ozaki_choice"] = choice
         outs[name] = Cm.cpu().numpy().copy() if rank == 0 and not args.no_cpu else None
 
     for gname, gprec, gdt, gsl in (("grouped_bf16x3", "bf16x3", torch.float32, 0),
@@ -604,13 +801,20 @@ def main():
             results[gname] = grouped_bench(cc, gprec, gdt, gsl, max(3, args.steps), args.warmup, seed=5 + 10 * rank)
     if not args.only or "fwd_bwd" in args.only.split(","):
         results["fwd_bwd_bf16x3"] = fwd_bwd_bench(cc, max(3, args.steps), args.warmup)
+        results["fwd_bwd_bf16x6"] = fwd_bwd_bench(cc, max(3, args.steps), args.warmup, precision="bf16x6")
+    if (not args.only or "spread" in args.only.split(",")) and rank == 0:
+        results["spread"] = spread_bench(cc, n, pk, sms, max(2, args.family_steps), 1, no_cpu=args.no_cpu)
+    if (not args.only and not args.no_families) or "families" in args.only.split(","):
+        results["families"] = families_bench(cc, pk, sms, args.family_steps, 1)
     avail = [p for p in paths if results.get(p[0], {}).get("available")]
     if not avail:  # a profiling run of the grouped launches only
         clocks = sampler.stop()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "results": results, "clocks": clocks}), flush=True)
         return 0
-    head_path = next((p for p in avail if p[0] == "bf16x3"), avail[0])
+    # Headline: the FP32-accurate tensor-core form (BF16x6: error at or below
+    # native FP32's); BF16x3 is reported beside it with its larger error.
+    head_path = next((p for p in avail if p[0] == "bf16x6"), avail[0])
     head, hA, hB, hC, hslices = head_path
     hprec = "native" if head.startswith("native") else head
     hr = results[head]
@@ -627,6 +831,7 @@ def main():
         cpu, errs = cpu_sample(n, A32.cpu().numpy(), B32.cpu().numpy(), A64.cpu().numpy(), B64.cpu().numpy(), outs)
         for name, e in errs.items():
             results[name]["error_vs_fp64"] = e
+        cpu["p1024"] = cpu_1024()
 
     # roofline of the headline's main kernel (useful flops / kernel time)
     kern_ms = hr.get("kernel_ms") or hr["ms"]
@@ -635,7 +840,7 @@ def main():
             "peak": hr["peak_tflops"], "unit": "TFLOP/s", "frac": achieved / hr["peak_tflops"],
             "traffic": dram_traffic(head, n),
             "peak_source": pk["source"] + ": " + hr["peak"], "kernel_ms": kern_ms}
-    dtypes = {"bf16x3": "bf16x3->f32", "bf16x6": "bf16x6->f32", "native_f32": "f32", "ozaki": "i8x%d->f64" % hslices,
+    dtypes = {"bf16x3": "bf16x3->f32", "bf16x6": "bf16x6->f32", "native_f32": "f32", "ozaki": "i8->f64",
               "native_f64": "f64"}
 
     if rank == 0:
