@@ -116,6 +116,16 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
       : "memory");
 }
 
+// 4-byte asynchronous copy global -> shared (no register is written; many
+// may be in flight per thread), and the wait for all of this thread's.
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(reinterpret_cast<uint64_t>(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // ------------------------------------------------------------------- tcgen05
 // TMEM allocation: one full warp executes alloc; the TMEM base address is
 // written to *dst (shared memory).  ncols is a power of two >= 32.

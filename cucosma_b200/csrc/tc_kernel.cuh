@@ -496,60 +496,72 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
 struct EpiF32 {
   static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
 
-  // Stores the 32 x 32 block staged in stg (row r of the warp's rows in
-  // stg[r * 33 + ...]) at columns col0 + c0 + [0, 32): coalesced rows.  When
-  // beta != 0 the C values of G rows are read together before those rows are
-  // written, so a block costs 32 / G read latencies instead of one a row (a
-  // store may alias the next row's read, so the reads are not reordered
-  // across the stores otherwise).  G trades registers for latency.
-  template <int G>
-  static __device__ __forceinline__ void store32(const OutCtx& p, const float* stg, int lane, int row0, int col,
-                                                 int z) {
-    if (col >= p.n) return;
+  // Writes one 32 x 32 block of results: acc[j] is this lane's row (row0 +
+  // lane) at column col + j.  With beta != 0 the C block is first copied into
+  // stg by cp.async (lanes = columns, all 32 rows in flight at once, so the
+  // block costs one memory latency; C was prefetched into L2), each lane
+  // combines its row from stg, and the results leave through stg as
+  // coalesced 128-byte row stores (lanes = columns).  Split-K partials are
+  // stored raw.  stg is a padded 32 x 33 tile (row r at r * 33), so both the
+  // row and the column accesses are free of bank conflicts.
+  static __device__ __forceinline__ void store_block(const OutCtx& p, float* o, const float (&acc)[32], float* stg,
+                                                     int lane, int row0, int col) {
+    if (col >= p.n) return;  // the whole block lies right of C (col is the block's first column)
+    const int cl = col + lane;  // this lane's column in the store pass
     if (p.partial) {
-      float* w = reinterpret_cast<float*>(p.out) + (int64_t)z * p.ws_split_stride + col;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = acc[j];
+    } else {
+      const float alpha = (float)p.alpha, beta = (float)p.beta;
+      if (beta != 0.f) {
+#pragma unroll 4
+        for (int r = 0; r < 32; ++r) {
+          const int row = row0 + r;
+          if (row < p.m && cl < p.n)
+            cp_async4(&stg[r * 33 + lane], o + (int64_t)row * p.ldo + cl);
+          else
+            stg[r * 33 + lane] = 0.f;
+        }
+        cp_async_wait_all();
+        __syncwarp();
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const float c = beta != 0.f ? stg[lane * 33 + j] : 0.f;
+        stg[lane * 33 + j] = apply_epi(combine(acc[j], alpha, beta, &c), p.epilogue);
+      }
+    }
+    __syncwarp();
+    if (cl < p.n) {
+      float* w = o + cl;
+      const int64_t ld = p.ldo;
 #pragma unroll 4
       for (int r = 0; r < 32; ++r) {
         const int row = row0 + r;
-        if (row < p.m) w[(int64_t)row * p.ldo] = stg[r * 33 + lane];
-      }
-    } else {
-      const float alpha = (float)p.alpha, beta = (float)p.beta;
-      float* o = reinterpret_cast<float*>(p.out) + col;
-#pragma unroll 1
-      for (int g = 0; g < 32; g += G) {
-        float c[G];
-#pragma unroll
-        for (int r = 0; r < G; ++r)
-          c[r] = beta != 0.f && row0 + g + r < p.m ? o[(int64_t)(row0 + g + r) * p.ldo] : 0.f;
-#pragma unroll
-        for (int r = 0; r < G; ++r) {
-          const int row = row0 + g + r;
-          if (row < p.m)
-            o[(int64_t)row * p.ldo] = apply_epi(combine(stg[(g + r) * 33 + lane], alpha, beta, &c[r]), p.epilogue);
-        }
+        if (row < p.m) w[(int64_t)row * ld] = stg[r * 33 + lane];
       }
     }
+    __syncwarp();
   }
 
   template <int BN>
   static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
                                              int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
+    float* o = reinterpret_cast<float*>(p.out) + (p.partial ? (int64_t)z * p.ws_split_stride : 0);
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t v0[16], v1[16];
       tmem_ld16(tacc + c0, v0);
       tmem_ld16(tacc + c0 + 16, v1);
       tmem_ld_wait();
+      float acc[32];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        stg[lane * 33 + j] = __uint_as_float(v0[j]);
-        stg[lane * 33 + 16 + j] = __uint_as_float(v1[j]);
+        acc[j] = __uint_as_float(v0[j]);
+        acc[16 + j] = __uint_as_float(v1[j]);
       }
-      __syncwarp();
-      store32<16>(p, stg, lane, row0, col0 + c0 + lane, z);
-      __syncwarp();
+      store_block(p, o, acc, stg, lane, row0, col0 + c0);
     }
   }
 
@@ -594,13 +606,13 @@ struct EpiF32 {
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[BN], uint8_t* stg_raw,
                                                 int lane, int row0, int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
+    float* o = reinterpret_cast<float*>(p.out) + (p.partial ? (int64_t)z * p.ws_split_stride : 0);
 #pragma unroll
     for (int c0 = 0; c0 < BN; c0 += 32) {
+      float acc[32];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = master[c0 + j];
-      __syncwarp();
-      store32<8>(p, stg, lane, row0, col0 + c0 + lane, z);  // master[] holds most registers: 8 C rows at a time
-      __syncwarp();
+      for (int j = 0; j < 32; ++j) acc[j] = master[c0 + j];
+      store_block(p, o, acc, stg, lane, row0, col0 + c0);
     }
   }
 };
@@ -824,6 +836,15 @@ struct Bf16x6Pair : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromot
 struct Bf16x6PairWide : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true, true> {
   static constexpr TermTable<6> kTerms{
       {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
+};
+
+// BF16x8: the six products of BF16x6 plus (1,2) and (2,1), so only lo * lo
+// (about 2^-34 of a product) is dropped; same tile and protocol.
+struct Bf16x8PairWide : TraitsBase<8, 256, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true, true> {
+  static constexpr TermTable<8> kTerms{{2, 1, 2, 1, 1, 0, 0, 0},
+                                       {1, 2, 0, 1, 0, 2, 1, 0},
+                                       {1, 1, 1, 1, 1, 1, 1, 0},
+                                       {true, false, false, false, false, false, false, true}};
 };
 
 // Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into
