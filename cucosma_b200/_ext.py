@@ -10,10 +10,11 @@ class TuneResult(C.Structure):
 
     _fields_ = [("split_k", C.c_int32), ("swizzle", C.c_int32), ("tile", C.c_int32), ("candidates", C.c_int32),
                 ("occupancy", C.c_int32), ("reserved", C.c_int32), ("ms", C.c_double), ("tflops", C.c_double),
-                ("l2_reuse_model", C.c_double)]
+                ("l2_hit_rate", C.c_double), ("dram_bytes", C.c_double), ("counter_passes", C.c_int32),
+                ("reserved2", C.c_int32)]
 
     def as_dict(self):
-        return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "reserved"}
+        return {f[0]: getattr(self, f[0]) for f in self._fields_ if not f[0].startswith("reserved")}
 
 
 class Problem(C.Structure):

@@ -41,7 +41,8 @@ enum Variant : int {
   kV6Pair = 5,       // BF16x6 256 x 128 CTA pair, two double-buffered accumulators (tile id 2)
   kV6PairWide = 6,   // BF16x6 256 x 256 CTA pair, two accumulators, split release (tile id 3)
   kVOzaki = 7,
-  kV8PairWide = 8,   // BF16x6 tile id 4: the 3-way split with eight products (BF16x8), 256 x 256 pair
+  kV6PairC4 = 8,     // BF16x6 256 x 256 pair promoted every 4 k-blocks (tile id 5)
+  kV6PairC2 = 9,     // BF16x6 256 x 256 pair promoted every 2 k-blocks (tile id 6)
 };
 
 // Tiling of one kernel: tiles, K blocks and splits, raster band.
@@ -129,14 +130,16 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
         case 1: pl.variant = kV6Single; break;
         case 2: pl.variant = kV6Pair; break;
         case 3: pl.variant = kV6PairWide; break;
-        case 4: pl.variant = kV8PairWide; break;
+        case 5: pl.variant = kV6PairC4; break;
+        case 6: pl.variant = kV6PairC2; break;
         default: pl.variant = pair_ok ? kV6PairWide : kV6Single;
       }
     }
     bn = (pl.variant == kV3Small || pl.variant == kV6Single || pl.variant == kV6Pair) ? 128 : 256;
     pl.kpad = round_up(K, 8);
   }
-  pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.variant == kV8PairWide)
+  pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.variant == kV6PairC4 ||
+             pl.variant == kV6PairC2)
                 ? 1
                 : 0;
   pl.tile_m = pl.pair ? 256 : 128;
@@ -345,8 +348,11 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
       case kV6PairWide:
         e = launch<Bf16x6PairWide>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWide>(di->sms)), st);
         break;
-      case kV8PairWide:
-        e = launch<Bf16x8PairWide>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x8PairWide>(di->sms)), st);
+      case kV6PairC4:
+        e = launch<Bf16x6PairWideC<4>>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWideC<4>>(di->sms)), st);
+        break;
+      case kV6PairC2:
+        e = launch<Bf16x6PairWideC<2>>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWideC<2>>(di->sms)), st);
         break;
       case kV3Small: e = launch<Bf16x3Promoted>(ta, tb, p, grid, st); break;
       case kV3Wide: e = launch<Bf16x3Wide>(ta, tb, p, grid, st); break;

@@ -838,13 +838,12 @@ struct Bf16x6PairWide : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, kPr
       {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
-// BF16x8: the six products of BF16x6 plus (1,2) and (2,1), so only lo * lo
-// (about 2^-34 of a product) is dropped; same tile and protocol.
-struct Bf16x8PairWide : TraitsBase<8, 256, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true, true> {
-  static constexpr TermTable<8> kTerms{{2, 1, 2, 1, 1, 0, 0, 0},
-                                       {1, 2, 0, 1, 0, 2, 1, 0},
-                                       {1, 1, 1, 1, 1, 1, 1, 0},
-                                       {true, false, false, false, false, false, false, true}};
+// The same tile promoted every CH k-blocks (a shorter chunk bounds how long
+// the tensor cores' truncating accumulation runs between promotions).
+template <int CH>
+struct Bf16x6PairWideC : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, CH, 8, 0, true, true> {
+  static constexpr TermTable<6> kTerms{
+      {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
 // Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into

@@ -5,15 +5,19 @@
 // split-K on the host and ranked them by a communication-volume model; the
 // thesis found that model a poor predictor and named occupancy and L2 hit rate
 // as what matters (thesis p.41-42).  Here the candidates -- split-K factor,
-// raster band / block-index remap width, and tile variant -- are run on the
-// device on the caller's buffers and ranked by measured time.  Each result
-// records the chosen kernel's occupancy (CUDA occupancy API) and a model of
-// the L2 reuse its raster achieves.  The winner is stored in a process-wide
-// cache keyed by (SM count, dtype, precision, slices, m, n, k); cucosma_gemm
-// consults it whenever the descriptor leaves split_k, swizzle and tile at 0.
-// The cache persists as a text file (cucosma_tune_cache_save / _load; loaded
-// automatically from $CUCOSMA_TUNE_CACHE on first use; CUCOSMA_TUNE=off
-// disables lookups).
+// raster band / block-index remap width, and tile variant (including the
+// 256-row CTA-pair tiles of the tensor-core paths) -- are run on the device on
+// the caller's buffers and ranked by measured time.  Each result records the
+// chosen kernel's occupancy (CUDA occupancy API) and the L2 hit rate and DRAM
+// bytes its tiling and raster achieve, read from the hardware counters with
+// the CUPTI range profiler (l2probe.cu; -1 when profiling is unavailable).
+// The winner is stored in a process-wide cache keyed by (SM count, dtype,
+// precision, slices, m, n, k); cucosma_gemm consults it whenever the
+// descriptor leaves split_k, swizzle and tile at 0, and the grouped planner
+// consults the grouped entries (cucosma_tune_grouped).  The cache persists as
+// a text file (cucosma_tune_cache_save / _load; loaded automatically from
+// $CUCOSMA_TUNE_CACHE on first use; CUCOSMA_TUNE=off disables lookups;
+// CUCOSMA_TUNE_COUNTERS=off skips the counter reading).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -26,6 +30,7 @@
 #include "api_internal.cuh"
 #include "simt_gemm.cuh"
 #include "skinny.cuh"
+#include "l2probe.cuh"
 
 namespace cucosma {
 namespace {
@@ -34,6 +39,8 @@ using Key = std::tuple<int, int, int, int, int64_t, int64_t, int64_t>;  // sms d
 struct Val {
   int split_k, swizzle, tile;
   double ms;
+  double l2_hit;      // measured L2 hit rate (percent), -1 when not measured
+  double dram_bytes;  // measured DRAM bytes read + written per call, -1 when not measured
 };
 
 std::mutex g_mu;
@@ -52,14 +59,23 @@ bool lookups_enabled() {
 cucosma_status load_locked(const char* path) {
   FILE* f = std::fopen(path, "r");
   if (!f) return CUCOSMA_STATUS_INVALID_VALUE;
-  char tag[16];
-  int sms, dt, pr, sl, sk, sw, ti;
-  long long m, n, k;
-  double ms;
-  while (std::fscanf(f, "%15s %d %d %d %d %lld %lld %lld %d %d %d %lf", tag, &sms, &dt, &pr, &sl, &m, &n, &k, &sk, &sw,
-                     &ti, &ms) == 12) {
-    if (std::strcmp(tag, "v1") != 0) continue;
-    g_cache[Key(sms, dt, pr, sl, m, n, k)] = Val{sk, sw, ti, ms};
+  // Lines: "v1 sms dtype precision slices m n k split_k swizzle tile ms" or
+  // "v2 ... ms l2_hit dram_bytes" (v2 adds the counter readings).
+  char line[512];
+  while (std::fgets(line, sizeof line, f)) {
+    char tag[16];
+    int sms, dt, pr, sl, sk, sw, ti;
+    long long m, n, k;
+    double ms, l2 = -1.0, dram = -1.0;
+    const int got = std::sscanf(line, "%15s %d %d %d %d %lld %lld %lld %d %d %d %lf %lf %lf", tag, &sms, &dt, &pr, &sl,
+                                &m, &n, &k, &sk, &sw, &ti, &ms, &l2, &dram);
+    if (got < 12) continue;
+    if (std::strcmp(tag, "v1") == 0) {
+      l2 = dram = -1.0;
+    } else if (std::strcmp(tag, "v2") != 0 || got != 14) {
+      continue;
+    }
+    g_cache[Key(sms, dt, pr, sl, m, n, k)] = Val{sk, sw, ti, ms, l2, dram};
   }
   std::fclose(f);
   return CUCOSMA_STATUS_SUCCESS;
@@ -78,17 +94,6 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-// Fraction of operand-tile loads a wave can serve from L2 under a banded
-// raster of height `band`: a wave of `ctas` tiles touches `band` row tiles of A
-// and ctas/band column tiles of B per k-block.  A model, not a measurement.
-double l2_reuse_model(int tiles_m, int tiles_n, int ctas, int band, double a_tile, double b_tile) {
-  const int wave = std::max(1, std::min(ctas, tiles_m * tiles_n));
-  const int rows = std::max(1, std::min({band, tiles_m, wave}));
-  const int cols = std::max(1, std::min(tiles_n, (wave + rows - 1) / rows));
-  const double loaded = (double)wave * (a_tile + b_tile);
-  const double distinct = rows * a_tile + cols * b_tile;
-  return loaded > 0 ? std::max(0.0, 1.0 - distinct / loaded) : 0.0;
-}
 
 }  // namespace
 
@@ -141,7 +146,10 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
     }
   } else {
     bands = {8, 4, 16};
-    if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = {0, 1, 2};
+    // tensor-core tiles: BF16x3 128x128, 128x256, 256x256 (CTA pair);
+    // BF16x6 128x128, 256x128 (pair), 256x256 (pair); Ozaki one tile per slice count
+    if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = {2, 3, 4};
+    if (d->precision == CUCOSMA_PRECISION_BF16X6) tiles = {1, 2, 3};
   }
   struct Cand {
     int sk, sw, ti;
@@ -186,10 +194,28 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (measured == 0) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
+  // Hardware counters of the chosen configuration (one profiled call per
+  // counter pass).
+  CounterReading cr{};
+  cr.l2_hit_pct = -1.0;
+  {
+    const char* e = std::getenv("CUCOSMA_TUNE_COUNTERS");
+    if (!(e && std::strcmp(e, "off") == 0)) {
+      cucosma_gemm_desc t = base;
+      t.split_k = pick.sk;
+      t.swizzle = pick.sw;
+      t.tile = pick.ti;
+      measure_counters([&] { return gemm(&t, A, B, C, workspace, workspace_bytes, st) == CUCOSMA_STATUS_SUCCESS; }, st,
+                       &cr);
+    } else {
+      cr.why = "disabled by CUCOSMA_TUNE_COUNTERS=off";
+    }
+  }
+  const double dram = cr.l2_hit_pct >= 0.0 ? cr.dram_read_bytes + cr.dram_write_bytes : -1.0;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     load_env_locked();
-    g_cache[key_of(d, di->sms)] = Val{pick.sk, pick.sw, pick.ti, best};
+    g_cache[key_of(d, di->sms)] = Val{pick.sk, pick.sw, pick.ti, best, cr.l2_hit_pct, dram};
   }
   if (out) {
     std::memset(out, 0, sizeof(*out));
@@ -210,12 +236,9 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
                                                  : simt::occupancy<double>();
     else
       out->occupancy = 1;  // persistent kernel, one CTA per SM by construction
-    const int es = d->precision == CUCOSMA_PRECISION_NATIVE ? (d->dtype == CUCOSMA_R_32F ? 4 : 8)
-                   : d->precision == CUCOSMA_PRECISION_OZAKI ? pk.slices
-                                                             : 2 * pk.slices;
-    const int64_t tiles_m = (d->m + pk.tile_m - 1) / pk.tile_m, tiles_n = (d->n + pk.tile_n - 1) / pk.tile_n;
-    out->l2_reuse_model = l2_reuse_model((int)tiles_m, (int)tiles_n, di->sms * std::max(1, out->occupancy),
-                                         std::max(1, pk.band), (double)pk.tile_m * es, (double)pk.tile_n * es);
+    out->l2_hit_rate = cr.l2_hit_pct;
+    out->dram_bytes = dram;
+    out->counter_passes = cr.passes;
   }
   return CUCOSMA_STATUS_SUCCESS;
 }
@@ -227,9 +250,10 @@ extern "C" cucosma_status cucosma_tune_cache_save(const char* path) {
   if (!f) return CUCOSMA_STATUS_INVALID_VALUE;
   for (const auto& kv : g_cache) {
     const Key& k = kv.first;
-    std::fprintf(f, "v1 %d %d %d %d %lld %lld %lld %d %d %d %.6f\n", std::get<0>(k), std::get<1>(k), std::get<2>(k),
-                 std::get<3>(k), (long long)std::get<4>(k), (long long)std::get<5>(k), (long long)std::get<6>(k),
-                 kv.second.split_k, kv.second.swizzle, kv.second.tile, kv.second.ms);
+    std::fprintf(f, "v2 %d %d %d %d %lld %lld %lld %d %d %d %.6f %.3f %.0f\n", std::get<0>(k), std::get<1>(k),
+                 std::get<2>(k), std::get<3>(k), (long long)std::get<4>(k), (long long)std::get<5>(k),
+                 (long long)std::get<6>(k), kv.second.split_k, kv.second.swizzle, kv.second.tile, kv.second.ms,
+                 kv.second.l2_hit, kv.second.dram_bytes);
   }
   std::fclose(f);
   return CUCOSMA_STATUS_SUCCESS;

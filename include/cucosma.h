@@ -178,7 +178,12 @@ typedef struct cucosma_tune_result {
   int32_t occupancy;              /* resident CTAs per SM of the chosen kernel */
   int32_t reserved;
   double ms, tflops;              /* measured time of one call of the chosen configuration */
-  double l2_reuse_model;          /* modelled fraction of operand-tile loads served by L2 */
+  double l2_hit_rate;             /* L2 hit rate (percent) of one call of it, read from the hardware
+                                   * counters (lts__t_sector_hit_rate, CUPTI range profiler); -1 when
+                                   * profiling is unavailable or CUCOSMA_TUNE_COUNTERS=off */
+  double dram_bytes;              /* DRAM bytes read + written by that call (counters), -1 likewise */
+  int32_t counter_passes;         /* profiled calls the counter reading took */
+  int32_t reserved2;
 } cucosma_tune_result;
 CUCOSMA_API cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A, const void* B, void* C,
                                         void* workspace, size_t workspace_bytes, int max_candidates,
