@@ -10,7 +10,8 @@ import cucosma_b200 as cc
 import oracle
 from tests._util import check_against_oracle, to_dev, uniform
 
-LINES = ["v1 148 0 0 0 1024 1024 1024 3 1 0 0.123000", "v1 148 0 1 0 8192 8192 8192 1 8 0 2.500000"]
+LINES = ["v2 148 0 0 0 1024 1024 1024 3 1 0 0.123000 71.250 12582912",
+         "v2 148 0 1 0 8192 8192 8192 1 8 4 2.500000 -1.000 -1"]
 
 
 def test_cache_file_roundtrip(tmp_path):
@@ -24,6 +25,20 @@ def test_cache_file_roundtrip(tmp_path):
     assert sorted(out.read_text().strip().splitlines()) == sorted(LINES)
     cc.tune_cache_clear()
     assert cc.tune_cache_size() == 0
+
+
+def test_cache_reads_v1_lines(tmp_path):
+    """Cache files written before the counter readings (v1 lines) still load;
+    their entries carry no measurement (-1)."""
+    cc.tune_cache_clear()
+    src = tmp_path / "v1.txt"
+    src.write_text("v1 148 0 0 0 1024 1024 1024 3 1 0 0.123000\n")
+    cc.tune_cache_load(str(src))
+    assert cc.tune_cache_size() == 1
+    out = tmp_path / "out.txt"
+    cc.tune_cache_save(str(out))
+    assert out.read_text().strip() == "v2 148 0 0 0 1024 1024 1024 3 1 0 0.123000 -1.000 -1"
+    cc.tune_cache_clear()
 
 
 @pytest.mark.gpu
@@ -40,7 +55,10 @@ def test_tune_then_use(cuda, tmp_path, precision, dtype):
     r = cc.tune(dA, dB, scratch, 1.0, 0.5, precision=precision)
     print(precision, r)
     assert r["candidates"] >= 3 and r["ms"] > 0 and r["tflops"] > 0 and r["occupancy"] >= 1
-    assert 0.0 <= r["l2_reuse_model"] <= 1.0
+    # the L2 hit rate and DRAM traffic of the chosen configuration, read from
+    # the hardware counters (CUPTI range profiler) on this GPU
+    assert 0.0 <= r["l2_hit_rate"] <= 100.0 and r["counter_passes"] >= 1
+    assert r["dram_bytes"] > 0
     assert cc.tune_cache_size() == 1
     dC = to_dev(Cin)
     plan = cc.get_plan(cc.make_desc(dA, dB, dC, 1.0, 0.5, precision=precision))
