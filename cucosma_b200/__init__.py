@@ -316,12 +316,13 @@ def gemm_backward(A, B, Y, dY, dA=None, dB=None, alpha=1.0, precision="bf16x3", 
     return dA, dB
 
 
-def grouped(problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0):
+def grouped(problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0, tile=0):
     """Plan a grouped launch over [(A, B, C), ...] device tensors; call the
-    returned object to enqueue it (two or three kernels, graph-capturable)."""
+    returned object to enqueue it (two or three kernels, graph-capturable).
+    tile 0 takes the tuner's choice for this batch when it has one."""
     from ._ext import GroupedPlan
 
-    return GroupedPlan(problems, precision, alpha, beta, epilogue, slices)
+    return GroupedPlan(problems, precision, alpha, beta, epilogue, slices, tile)
 
 
 def set_wait_timeout_ns(ns):

@@ -34,6 +34,8 @@ def bind(L):
         "cucosma_grouped_plan_create": ([C.POINTER(GemmDesc), P, C.c_int, vp, sz, C.POINTER(vp)], C.c_int),
         "cucosma_gemm_grouped": ([vp, vp], C.c_int),
         "cucosma_grouped_plan_destroy": ([vp], C.c_int),
+        "cucosma_grouped_plan_get_tile": ([vp] + [C.POINTER(C.c_int32)] * 4, C.c_int),
+        "cucosma_tune_grouped": ([C.POINTER(GemmDesc), P, C.c_int, vp, sz, C.POINTER(TuneResult), vp], C.c_int),
         "cucosma_tune": ([C.POINTER(GemmDesc), vp, vp, vp, vp, sz, C.c_int, C.POINTER(TuneResult), vp], C.c_int),
         "cucosma_tune_cache_save": ([C.c_char_p], C.c_int),
         "cucosma_tune_cache_load": ([C.c_char_p], C.c_int),
@@ -57,7 +59,7 @@ class GroupedPlan:
     (A, B, C) row-major device tensors sharing dtype; the plan keeps them and
     its workspace alive.  __call__ enqueues the launch on the current stream."""
 
-    def __init__(self, problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0):
+    def __init__(self, problems, precision="bf16x3", alpha=1.0, beta=0.0, epilogue="none", slices=0, tile=0):
         import torch
 
         from . import EPILOGUES, PRECISIONS, GemmDesc, _dtype_code, _ld, check, lib
@@ -73,7 +75,8 @@ class GroupedPlan:
         d.dtype = _dtype_code(self.problems[0][2])
         d.precision = PRECISIONS[precision]
         d.epilogue = EPILOGUES[epilogue]
-        d.alpha, d.beta, d.slices = float(alpha), float(beta), int(slices)
+        d.alpha, d.beta, d.slices, d.tile = float(alpha), float(beta), int(slices), int(tile)
+        self.desc = d
         n = C.c_size_t(0)
         check(L.cucosma_grouped_workspace_size(C.byref(d), arr, len(self.problems), C.byref(n)),
               "cucosma_grouped_workspace_size")
@@ -89,6 +92,26 @@ class GroupedPlan:
         from . import _stream_handle, check
 
         check(self._lib.cucosma_gemm_grouped(self.handle, _stream_handle(stream)), "cucosma_gemm_grouped")
+
+    def tile(self):
+        """(tile id, tile rows, tile columns, whether it came from the tuning cache)."""
+        from . import check
+
+        v = [C.c_int32() for _ in range(4)]
+        check(self._lib.cucosma_grouped_plan_get_tile(self.handle, *[C.byref(x) for x in v]),
+              "cucosma_grouped_plan_get_tile")
+        return tuple(int(x.value) for x in v[:3]) + (bool(v[3].value),)
+
+    def tune(self, stream=None):
+        """cucosma_tune_grouped on this plan's problems (their C is
+        overwritten) and workspace; returns the result as a dict."""
+        from . import _stream_handle, check
+
+        r = TuneResult()
+        check(self._lib.cucosma_tune_grouped(C.byref(self.desc), self._arr, len(self.problems), self.workspace.data_ptr(),
+                                             self.workspace.numel(), C.byref(r), _stream_handle(stream)),
+              "cucosma_tune_grouped")
+        return r.as_dict()
 
     def close(self):
         if getattr(self, "handle", None):

@@ -72,6 +72,8 @@ void* managed_workspace(size_t bytes, cudaStream_t st);
 // Tuning cache (tune.cu): when d leaves split_k, swizzle and tile at 0 and the
 // cache holds a choice for it, returns tmp filled with that choice, else d.
 const cucosma_gemm_desc* apply_tuning(const cucosma_gemm_desc* d, cucosma_gemm_desc* tmp, const DeviceInfo* di);
+// The grouped tile the tuner chose for this batch of shapes (cucosma_tune_grouped), 0 if none.
+int grouped_tuned_tile(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr, int count, const DeviceInfo* di);
 
 // Launch accounting and optional timing of the main GEMM kernel of each call:
 // note_launches() counts every kernel the library enqueues; prof_begin /

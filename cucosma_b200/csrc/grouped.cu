@@ -21,6 +21,7 @@
 struct cucosma_grouped_plan_st {
   cucosma_gemm_desc desc;
   int count = 0, kind = 0, slices = 0, total_tiles = 0;
+  int tile = 1, tile_m = 128, tile_n = 128, pair = 0, from_cache = 0;
   int pre_a_blocks = 0, pre_b_blocks = 0, exp_a_blocks = 0, exp_b_blocks = 0;
   int device = 0;
   void* workspace = nullptr;
@@ -268,15 +269,41 @@ namespace {
 
 size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Tile of a grouped launch (descriptor tile id, 0 = the tuner's cached choice
+// for this batch, else 1):
+//   BF16X3  1 = 128 x 128 promoted, 2 = 128 x 256 promoted, 3 = 256 x 256 CTA pair
+//   BF16X6  1 = 128 x 128, 2 = 256 x 256 CTA pair (split release)
+//   OZAKI   1 = 128 x ozaki_bn(slices)
+struct GTile {
+  int id, tile_m, bn, pair;
+};
+bool grouped_tile(int kind, int slices, int id, GTile& g) {
+  if (id == 0) id = 1;
+  if (kind == 0 && id >= 1 && id <= 3) {
+    g = id == 1 ? GTile{1, 128, 128, 0} : id == 2 ? GTile{2, 128, 256, 0} : GTile{3, 256, 256, 1};
+    return true;
+  }
+  if (kind == 1 && id >= 1 && id <= 2) {
+    g = id == 1 ? GTile{1, 128, 128, 0} : GTile{2, 256, 256, 1};
+    return true;
+  }
+  if (kind == 2 && id == 1) {
+    g = GTile{1, 128, ozaki_bn(slices), 0};
+    return true;
+  }
+  return false;
+}
+
 struct Layout {
-  int kind, slices, bn;
+  int kind, slices, bn, tile_m, pair, tile;
   size_t table_bytes, total_bytes;
   std::vector<GroupEntry> entries;  // pointers relative to the workspace base (offsets)
   std::vector<size_t> off_a, off_b, off_ea, off_eb;
   int total_tiles, pre_a, pre_b, exp_a, exp_b;
 };
 
-cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr, int count, Layout& L) {
+cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr, int count, Layout& L,
+                      int tile = -1) {
   if (!d || !pr || count <= 0) return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->flags != 0 || d->epilogue < 0 || d->epilogue > CUCOSMA_EPILOGUE_RELU) return CUCOSMA_STATUS_INVALID_VALUE;
   if (d->precision == CUCOSMA_PRECISION_OZAKI) {
@@ -284,15 +311,19 @@ cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr
     L.kind = 2;
     L.slices = d->slices ? d->slices : kOzakiDefaultSlices;
     if (L.slices < 4 || L.slices > 9) return CUCOSMA_STATUS_NOT_SUPPORTED;
-    L.bn = ozaki_bn(L.slices);
   } else if (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6) {
     if (d->dtype != CUCOSMA_R_32F) return CUCOSMA_STATUS_NOT_SUPPORTED;
     L.kind = d->precision == CUCOSMA_PRECISION_BF16X6 ? 1 : 0;
     L.slices = L.kind == 1 ? 3 : 2;
-    L.bn = 128;
   } else {
     return CUCOSMA_STATUS_NOT_SUPPORTED;  // the grouped launch is a tensor-core path
   }
+  GTile g{};
+  if (!grouped_tile(L.kind, L.slices, tile >= 0 ? tile : d->tile, g)) return CUCOSMA_STATUS_NOT_SUPPORTED;
+  L.bn = g.bn;
+  L.tile_m = g.tile_m;
+  L.pair = g.pair;
+  L.tile = g.id;
   const int es_in = L.kind == 2 ? 8 : 4;
   const int es_pl = L.kind == 2 ? 1 : 2;
   const int64_t kmax_exact = ((int64_t)2147483647 / ((int64_t)L.slices * 127 * 127)) / 32 * 32;
@@ -325,7 +356,7 @@ cucosma_status layout(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr
     e.k = (int)q.k;
     e.kpad = L.kind == 2 ? round_up(q.k, 32) : round_up(q.k, 8);
     e.kblocks = (int)ceil_div(q.k, 32);
-    e.tiles_m = (int)ceil_div(q.m, 128);
+    e.tiles_m = (int)ceil_div(q.m, L.tile_m);
     e.tiles_n = (int)ceil_div(q.n, L.bn);
     e.tile_start = tiles;
     tiles += e.tiles_m * e.tiles_n;
@@ -387,14 +418,20 @@ extern "C" cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d
                                                       cucosma_grouped_plan* plan) {
   if (!plan) return CUCOSMA_STATUS_INVALID_VALUE;
   *plan = nullptr;
-  Layout L;
-  cucosma_status s = layout(d, problems, count, L);
-  if (s != CUCOSMA_STATUS_SUCCESS) return s;
-  if (!workspace || workspace_bytes < L.total_bytes) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
-  if (reinterpret_cast<uintptr_t>(workspace) & 255) return CUCOSMA_STATUS_MISALIGNED;
   const DeviceInfo* di = device_info();
   if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
   if (di->cc_major != 10 || di->cc_minor != 0) return CUCOSMA_STATUS_ARCH_MISMATCH;
+  // tile 0: the tuner's choice for this batch of shapes, when it has one
+  int tile = d ? d->tile : 0, from_cache = 0;
+  if (d && tile == 0) {
+    tile = grouped_tuned_tile(d, problems, count, di);
+    from_cache = tile > 0;
+  }
+  Layout L;
+  cucosma_status s = layout(d, problems, count, L, tile);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  if (!workspace || workspace_bytes < L.total_bytes) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
+  if (reinterpret_cast<uintptr_t>(workspace) & 255) return CUCOSMA_STATUS_MISALIGNED;
   uint8_t* w = static_cast<uint8_t*>(workspace);
   for (int i = 0; i < count; ++i) {
     GroupEntry& e = L.entries[i];
@@ -414,7 +451,7 @@ extern "C" cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d
       ok = encode_3d(&e.tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, e.planes_a, e.k, e.m, s_, e.kpad,
                      (uint64_t)e.m * e.kpad, 32, 128, s_, CU_TENSOR_MAP_SWIZZLE_64B) &&
            encode_3d(&e.tmB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, e.planes_b, e.k, e.n, s_, e.kpad,
-                     (uint64_t)e.n * e.kpad, 32, L.bn, s_, CU_TENSOR_MAP_SWIZZLE_64B);
+                     (uint64_t)e.n * e.kpad, 32, L.pair ? L.bn / 2 : L.bn, s_, CU_TENSOR_MAP_SWIZZLE_64B);
     }
     if (!ok) return CUCOSMA_STATUS_LAUNCH_FAILED;
   }
@@ -427,6 +464,11 @@ extern "C" cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d
   p->kind = L.kind;
   p->slices = L.slices;
   p->total_tiles = L.total_tiles;
+  p->tile = L.tile;
+  p->tile_m = L.tile_m;
+  p->tile_n = L.bn;
+  p->pair = L.pair;
+  p->from_cache = from_cache;
   p->pre_a_blocks = L.pre_a;
   p->pre_b_blocks = L.pre_b;
   p->exp_a_blocks = L.exp_a;
@@ -440,6 +482,16 @@ extern "C" cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* d
 
 extern "C" cucosma_status cucosma_grouped_plan_destroy(cucosma_grouped_plan plan) {
   delete plan;
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
+extern "C" cucosma_status cucosma_grouped_plan_get_tile(cucosma_grouped_plan plan, int32_t* tile, int32_t* tile_m,
+                                                       int32_t* tile_n, int32_t* from_cache) {
+  if (!plan) return CUCOSMA_STATUS_INVALID_VALUE;
+  if (tile) *tile = plan->tile;
+  if (tile_m) *tile_m = plan->tile_m;
+  if (tile_n) *tile_n = plan->tile_n;
+  if (from_cache) *from_cache = plan->from_cache;
   return CUCOSMA_STATUS_SUCCESS;
 }
 
@@ -483,8 +535,16 @@ extern "C" cucosma_status cucosma_gemm_grouped(cucosma_grouped_plan plan, void* 
       grouped_split_bf16_kernel<2><<<blocks, 256, 0, st>>>(plan->table, plan->count, plan->pre_a_blocks);
     e = cudaGetLastError();
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    auto pair_grid = [&](int clusters) { return 2 * std::max(1, std::min(plan->total_tiles, clusters)); };
     prof_begin(st);
-    e = plan->kind == 1 ? launch<Bf16x6>(dummy, dummy, p, grid, st) : launch<Bf16x3Promoted>(dummy, dummy, p, grid, st);
+    if (plan->kind == 1)
+      e = plan->tile == 2
+              ? launch<Bf16x6PairWide>(dummy, dummy, p, pair_grid(max_pair_clusters<Bf16x6PairWide>(di->sms)), st)
+              : launch<Bf16x6>(dummy, dummy, p, grid, st);
+    else
+      e = plan->tile == 3   ? launch<Bf16x3Pair>(dummy, dummy, p, pair_grid(max_pair_clusters<Bf16x3Pair>(di->sms)), st)
+          : plan->tile == 2 ? launch<Bf16x3>(dummy, dummy, p, grid, st)
+                            : launch<Bf16x3Promoted>(dummy, dummy, p, grid, st);
     prof_end(st);
     note_launches(2);
   } else {

@@ -97,6 +97,34 @@ double elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
 
 }  // namespace
 
+// Grouped entries: the key's m is -count and n a 62-bit FNV-1a hash of the
+// problems' (m, n, k) in order (k = -1 marks the entry), so a batch is found
+// again by its shape mix.
+static Key grouped_key(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr, int count, int sms) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](int64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      h ^= (uint64_t)((v >> (8 * b)) & 0xff);
+      h *= 1099511628211ull;
+    }
+  };
+  mix(count);
+  for (int i = 0; i < count; ++i) {
+    mix(pr[i].m);
+    mix(pr[i].n);
+    mix(pr[i].k);
+  }
+  return Key(sms, d->dtype, d->precision, d->slices, -(int64_t)count, (int64_t)(h >> 2), -1);
+}
+
+int grouped_tuned_tile(const cucosma_gemm_desc* d, const cucosma_gemm_problem* pr, int count, const DeviceInfo* di) {
+  if (!d || !pr || count <= 0 || !di || !lookups_enabled()) return 0;
+  std::lock_guard<std::mutex> lk(g_mu);
+  load_env_locked();
+  auto it = g_cache.find(grouped_key(d, pr, count, di->sms));
+  return it == g_cache.end() ? 0 : it->second.tile;
+}
+
 const cucosma_gemm_desc* apply_tuning(const cucosma_gemm_desc* d, cucosma_gemm_desc* tmp, const DeviceInfo* di) {
   if (!d || !di || d->split_k || d->swizzle || d->tile || !lookups_enabled()) return d;
   std::lock_guard<std::mutex> lk(g_mu);
@@ -236,6 +264,87 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
                                                  : simt::occupancy<double>();
     else
       out->occupancy = 1;  // persistent kernel, one CTA per SM by construction
+    out->l2_hit_rate = cr.l2_hit_pct;
+    out->dram_bytes = dram;
+    out->counter_passes = cr.passes;
+  }
+  return CUCOSMA_STATUS_SUCCESS;
+}
+
+extern "C" cucosma_status cucosma_tune_grouped(const cucosma_gemm_desc* d, const cucosma_gemm_problem* problems,
+                                               int count, void* workspace, size_t workspace_bytes,
+                                               cucosma_tune_result* out, void* stream) {
+  if (!d || !problems || count <= 0) return CUCOSMA_STATUS_INVALID_VALUE;
+  const DeviceInfo* di = device_info();
+  if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // Candidate tiles of the grouped launch (see cucosma_grouped_plan_create).
+  std::vector<int> tiles;
+  if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = {1, 2, 3};
+  else if (d->precision == CUCOSMA_PRECISION_BF16X6) tiles = {1, 2};
+  else tiles = {1};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  double best = 1e300;
+  int pick = 0, measured = 0;
+  cucosma_status s = CUCOSMA_STATUS_SUCCESS;
+  for (int ti : tiles) {
+    cucosma_gemm_desc t = *d;
+    t.tile = ti;
+    cucosma_grouped_plan plan = nullptr;
+    if (cucosma_grouped_plan_create(&t, problems, count, workspace, workspace_bytes, &plan) != CUCOSMA_STATUS_SUCCESS)
+      continue;
+    double tmin = 1e300;
+    bool ok = cucosma_gemm_grouped(plan, stream) == CUCOSMA_STATUS_SUCCESS;  // warm-up
+    for (int r = 0; ok && r < 3; ++r) {
+      cudaEventRecord(e0, st);
+      ok = cucosma_gemm_grouped(plan, stream) == CUCOSMA_STATUS_SUCCESS;
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        ok = false;
+        s = CUCOSMA_STATUS_LAUNCH_FAILED;
+      }
+      tmin = std::min(tmin, elapsed_ms(e0, e1));
+    }
+    cucosma_grouped_plan_destroy(plan);
+    if (!ok) continue;
+    ++measured;
+    if (tmin < best) {
+      best = tmin;
+      pick = ti;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s != CUCOSMA_STATUS_SUCCESS) return s;
+  if (measured == 0) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
+  CounterReading cr{};
+  cr.l2_hit_pct = -1.0;
+  const char* env = std::getenv("CUCOSMA_TUNE_COUNTERS");
+  if (!(env && std::strcmp(env, "off") == 0)) {
+    cucosma_gemm_desc t = *d;
+    t.tile = pick;
+    cucosma_grouped_plan plan = nullptr;
+    if (cucosma_grouped_plan_create(&t, problems, count, workspace, workspace_bytes, &plan) == CUCOSMA_STATUS_SUCCESS) {
+      measure_counters([&] { return cucosma_gemm_grouped(plan, stream) == CUCOSMA_STATUS_SUCCESS; }, st, &cr);
+      cucosma_grouped_plan_destroy(plan);
+    }
+  }
+  const double dram = cr.l2_hit_pct >= 0.0 ? cr.dram_read_bytes + cr.dram_write_bytes : -1.0;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_env_locked();
+    g_cache[grouped_key(d, problems, count, di->sms)] = Val{0, 0, pick, best, cr.l2_hit_pct, dram};
+  }
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->tile = pick;
+    out->candidates = measured;
+    out->occupancy = 1;
+    out->ms = best;
+    double flop = 0.0;
+    for (int i = 0; i < count; ++i) flop += 2.0 * (double)problems[i].m * (double)problems[i].n * (double)problems[i].k;
+    out->tflops = flop / (best * 1e-3) / 1e12;
     out->l2_hit_rate = cr.l2_hit_pct;
     out->dram_bytes = dram;
     out->counter_passes = cr.passes;

@@ -255,6 +255,24 @@ CUCOSMA_API cucosma_status cucosma_grouped_plan_create(const cucosma_gemm_desc* 
                                                        cucosma_grouped_plan* plan);
 CUCOSMA_API cucosma_status cucosma_gemm_grouped(cucosma_grouped_plan plan, void* stream);
 CUCOSMA_API cucosma_status cucosma_grouped_plan_destroy(cucosma_grouped_plan plan);
+/* The plan's tile: descriptor tile id (BF16X3 1 = 128 x 128 promoted,
+ * 2 = 128 x 256 promoted, 3 = 256 x 256 CTA pair; BF16X6 1 = 128 x 128,
+ * 2 = 256 x 256 pair; Ozaki 1), its rows and columns, and whether it came
+ * from the tuning cache (descriptor tile 0 with a cucosma_tune_grouped entry
+ * for this batch; otherwise tile 0 means 1). */
+CUCOSMA_API cucosma_status cucosma_grouped_plan_get_tile(cucosma_grouped_plan plan, int32_t* tile, int32_t* tile_m,
+                                                         int32_t* tile_n, int32_t* from_cache);
+
+/* The grouped launch's counterpart: its candidate tiles (BF16X3: 128 x 128,
+ * 128 x 256, 256 x 256 CTA pair; BF16X6: 128 x 128, 256 x 256 pair; Ozaki:
+ * one) are run on the problems (their C is overwritten) and the fastest is
+ * cached for this batch's shape mix (SM count, dtype, precision, slices and
+ * the problems' m, n, k in order).  cucosma_grouped_plan_create uses it when
+ * the descriptor's tile is 0.  out->tile is the chosen grouped tile id. */
+CUCOSMA_API cucosma_status cucosma_tune_grouped(const cucosma_gemm_desc* d, const cucosma_gemm_problem* problems,
+                                                int count, void* workspace, size_t workspace_bytes,
+                                                cucosma_tune_result* out, void* stream);
+
 
 /* Allocation-free FP32 split-K GEMM.  No counterpart in the reference (whose
  * split-K path cudaMallocs its workspace on every call).  For callers that

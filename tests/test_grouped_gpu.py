@@ -44,7 +44,8 @@ def single(A, B, Cin, precision, slices, alpha, beta):
     import torch
 
     dA, dB, dC = to_dev(A), to_dev(B), to_dev(Cin)
-    tile = 2 if precision == "bf16x3" else 0
+    # grouped tile 1 = the 128 x 128 tiles (BF16x3 promoted: single tile 2; BF16x6: single tile 1)
+    tile = 2 if precision == "bf16x3" else 1 if precision == "bf16x6" else 0
     cc.gemm(dA, dB, dC, alpha, beta, precision=precision, slices=slices, split_k=1, tile=tile)
     torch.cuda.synchronize()
     return dC.cpu().numpy()
@@ -166,3 +167,64 @@ def test_grouped_rejects_bad_input():
     arr[0] = cc._ext.Problem(8, 8, 8, 9, 8, 8, 0x10000, 0x10000, 0x10000)
     assert L.cucosma_grouped_workspace_size(C.byref(d), arr, 1, C.byref(n)) == cc.MISALIGNED
     assert L.cucosma_grouped_workspace_size(C.byref(d), arr, 0, C.byref(n)) == cc.INVALID_VALUE
+
+
+# grouped tile id -> the single-launch tile id with the same per-element arithmetic
+GROUPED_TILES = [("bf16x3", 1, 2), ("bf16x3", 2, 3), ("bf16x3", 3, 4), ("bf16x6", 1, 1), ("bf16x6", 2, 3)]
+
+
+@pytest.mark.parametrize("precision,gtile,stile", GROUPED_TILES,
+                         ids=["bf16x3-128x128", "bf16x3-128x256", "bf16x3-pair256", "bf16x6-128x128",
+                              "bf16x6-pair256"])
+def test_grouped_tiles_match_single_launches(precision, gtile, stile):
+    """Every grouped tile (CTA-pair tiles included) gives each problem's
+    result bit for bit as the single launch with the same tile."""
+    import torch
+
+    sh = shapes(3, 23, hi=700, khi=900) + [(1, 1, 1), (257, 129, 40), (600, 300, 77)]
+    host, dev = make(sh, np.float32, 300)
+    plan = cc.grouped(dev, precision=precision, alpha=1.0, beta=0.5, tile=gtile)
+    assert plan.tile()[:1] == (gtile,) and not plan.tile()[3]
+    plan()
+    torch.cuda.synchronize()
+    for (A, B, Cin), (_, _, dC) in zip(host, dev):
+        dA, dB, dS = to_dev(A), to_dev(B), to_dev(Cin)
+        cc.gemm(dA, dB, dS, 1.0, 0.5, precision=precision, split_k=1, tile=stile)
+        torch.cuda.synchronize()
+        assert np.array_equal(dC.cpu().numpy(), dS.cpu().numpy()), (A.shape, B.shape)
+
+
+def test_grouped_plan_takes_its_tile_from_the_tuner():
+    """cucosma_tune_grouped measures the grouped tiles on a batch and caches
+    the fastest for its shape mix; a plan created afterwards with tile 0 uses
+    that tile (reported as coming from the cache), its results equal a plan
+    with that tile given explicitly, and the measured L2 hit rate and DRAM
+    bytes of the chosen launch are reported."""
+    import torch
+
+    cc.tune_cache_clear()
+    try:
+        sh = shapes(4, 31, lo=64, hi=1024, klo=64, khi=2048)
+        _, dev = make(sh, np.float32, 400)
+        base = cc.grouped(dev, precision="bf16x3")
+        assert base.tile() == (1, 128, 128, False)
+        r = base.tune()
+        print("grouped tune:", r)
+        assert r["candidates"] == 3 and r["tile"] in (1, 2, 3) and r["ms"] > 0
+        assert 0.0 <= r["l2_hit_rate"] <= 100.0 and r["dram_bytes"] > 0
+        tuned = cc.grouped(dev, precision="bf16x3")
+        tid, tm, tn, from_cache = tuned.tile()
+        assert from_cache and tid == r["tile"]
+        tuned()
+        torch.cuda.synchronize()
+        got = [d[2].cpu().numpy().copy() for d in dev]
+        explicit = cc.grouped(dev, precision="bf16x3", tile=tid)
+        explicit()
+        torch.cuda.synchronize()
+        for g, d in zip(got, dev):
+            assert np.array_equal(g, d[2].cpu().numpy())
+        # another batch keeps the default tile
+        other = cc.grouped(dev[:-1], precision="bf16x3")
+        assert other.tile()[3] is False
+    finally:
+        cc.tune_cache_clear()
