@@ -55,7 +55,7 @@ class PlanInfo(C.Structure):
         ("kchunk", C.c_int64), ("kpad", C.c_int64),
         ("workspace_bytes", C.c_uint64), ("off_a", C.c_uint64), ("off_b", C.c_uint64), ("off_ea", C.c_uint64),
         ("off_eb", C.c_uint64), ("off_part", C.c_uint64), ("off_choice", C.c_uint64),
-        ("layout_slices", C.c_int32), ("reserved", C.c_int32),
+        ("layout_slices", C.c_int32), ("fused", C.c_int32),
     ]
 
     def as_dict(self):

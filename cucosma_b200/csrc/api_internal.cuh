@@ -49,7 +49,11 @@ bool encode_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const v
 
 // Tensor-core paths (BF16x3 / BF16x6 / Ozaki), tc_gemm.cu.
 cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, const DeviceInfo* di);
-void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info);
+// allow_fused = false: the plan of a call whose operand planes are prepared
+// by the caller (the fused-split kernel is then never chosen).
+void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info, bool allow_fused = true);
+// Whether a plain call with *d runs the fused-split kernel.
+bool tc_plan_is_fused(const cucosma_gemm_desc* d, const DeviceInfo* di);
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                        const DeviceInfo* di, cudaStream_t st);
 // prep: which operand pre-passes run (kPrepA | kPrepB for a plain call).  An

@@ -112,7 +112,7 @@ extern "C" cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* f, cons
   // caller's workspace (the cache may have changed since it was sized).
   auto resolve = [&](cucosma_gemm_desc* d, cucosma_gemm_desc* tuned) -> const cucosma_gemm_desc* {
     const cucosma_gemm_desc* r = apply_tuning(d, tuned, di);
-    tc_plan_info(r, di, &pi);
+    tc_plan_info(r, di, &pi, false);  // the planes are prepared here: never the fused kernel
     return r;
   };
   if (dA) {

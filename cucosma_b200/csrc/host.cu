@@ -147,6 +147,20 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
   if (!h) return CUCOSMA_STATUS_LAUNCH_FAILED;
   CallEvents ev;
   if (!ev.create(L.blocks)) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  // When the first block runs the fused-split kernel it writes no B planes,
+  // so the later blocks prepare their own.
+  bool b_shared = true;
+  if (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6) {
+    const DeviceInfo* di = device_info();
+    if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+    cucosma_gemm_desc first = *d;
+    first.m = std::min<int64_t>(L.rows_per_block, d->m);
+    first.lda = L.lda;
+    first.ldb = L.ldb;
+    first.ldc = L.ldc;
+    cucosma_gemm_desc tuned;
+    b_shared = !tc_plan_is_fused(apply_tuning(&first, &tuned, di), di);
+  }
   const size_t es = d->dtype == CUCOSMA_R_32F ? 4 : 8;
   uint8_t* w = static_cast<uint8_t*>(device_buffer);
   uint8_t* dA = w + L.off_a;
@@ -184,7 +198,7 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
     sub.ldc = L.ldc;
     // B's operand planes: prepared by the first block, reused by the rest.
     s = gemm_ex(&sub, dA + r0 * L.lda * es, dB, dC + r0 * L.ldc * es, ws, L.ws_bytes, h->gemm,
-                i == 0 ? (kPrepA | kPrepB) : kPrepA);
+                (i == 0 || !b_shared) ? (kPrepA | kPrepB) : kPrepA);
     if (s != CUCOSMA_STATUS_SUCCESS) return s;
     if (fail(cudaEventRecord(ev.c_ready[i], h->gemm)) || fail(cudaStreamWaitEvent(h->out, ev.c_ready[i], 0)) ||
         fail(cudaMemcpy2DAsync(hC + r0 * d->ldc * es, d->ldc * es, dC + r0 * L.ldc * es, L.ldc * es, d->n * es, rows,

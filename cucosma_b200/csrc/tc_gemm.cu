@@ -2,6 +2,7 @@
 // paths (BF16x3, BF16x6, Ozaki); the kernel template is in tc_kernel.cuh.
 #include "simt_gemm.cuh"
 #include "split.cuh"
+#include "tc_fused.cuh"
 #include "tc_kernel.cuh"
 
 namespace cucosma {
@@ -43,6 +44,8 @@ enum Variant : int {
   kVOzaki = 7,
   kV6PairC4 = 8,     // BF16x6 256 x 256 pair promoted every 4 k-blocks (tile id 5)
   kV6PairC2 = 9,     // BF16x6 256 x 256 pair promoted every 2 k-blocks (tile id 6)
+  kV3Fused = 10,     // BF16x3 256 x 128 pair, split fused into the kernel (tile id 5)
+  kV6Fused = 11,     // BF16x6 256 x 128 pair, split fused into the kernel (tile id 4)
 };
 
 // Tiling of one kernel: tiles, K blocks and splits, raster band.
@@ -53,6 +56,7 @@ struct Tiling {
 struct Plan {
   int kind;  // 0 bf16x3, 1 bf16x6, 2 ozaki
   int variant, pair, tile_m, bn_local, bk;
+  int fused;         // BF16 split done inside the GEMM kernel (no planes in the workspace)
   Tiling t;          // the kernel (Ozaki adaptive: the 8-slice candidate)
   int adaptive;      // Ozaki with the slice count chosen on the device
   int layout_slices; // Ozaki slices per k-block in the workspace
@@ -98,7 +102,22 @@ static Tiling make_tiling(const Plan& pl, int slices, int bn, const cucosma_gemm
   return t;
 }
 
-static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
+// The fused split pays off when the separate pre-pass (read the FP32
+// operands, write nt BF16 planes) would take more than a quarter of the
+// GEMM's own bound (tensor time at nt products of BF16, or the HBM time of
+// reading the planes and writing -- with beta, also reading -- C): operands
+// read only a few times, as in the large-K and large-N families.
+static bool fused_pays(const cucosma_gemm_desc* d, int nt) {
+  const double M = (double)d->m, N = (double)d->n, K = (double)d->k;
+  const double hbm = 6.5e12, bf16 = 1.6e15;
+  const double products = nt == 2 ? 3.0 : 6.0;
+  const double t_pre = (M * K + K * N) * (4.0 + 2.0 * nt) / hbm;
+  const double t_mma = 2.0 * M * N * K * products / bf16;
+  const double t_mem = ((M * K + K * N) * 2.0 * nt + M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0)) / hbm;
+  return t_pre > 0.25 * std::max(t_mma, t_mem);
+}
+
+static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool allow_fused = true) {
   Plan pl{};
   const int64_t M = d->m, N = d->n, K = d->k;
   int slices = 0, bn = 0;
@@ -123,23 +142,31 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
         case 2: pl.variant = kV3Small; break;
         case 3: pl.variant = kV3Promoted; break;
         case 4: pl.variant = kV3Pair; break;
-        default: pl.variant = pair_ok ? kV3Pair : kV3Promoted;
+        case 5: pl.variant = allow_fused ? kV3Fused : kV3Pair; break;
+        default:
+          pl.variant = !pair_ok ? kV3Promoted : (allow_fused && fused_pays(d, 2)) ? kV3Fused : kV3Pair;
       }
     } else {
       switch (d->tile) {
         case 1: pl.variant = kV6Single; break;
         case 2: pl.variant = kV6Pair; break;
         case 3: pl.variant = kV6PairWide; break;
+        case 4: pl.variant = allow_fused ? kV6Fused : kV6Pair; break;
         case 5: pl.variant = kV6PairC4; break;
         case 6: pl.variant = kV6PairC2; break;
-        default: pl.variant = pair_ok ? kV6PairWide : kV6Single;
+        default:
+          pl.variant = !pair_ok ? kV6Single : (allow_fused && fused_pays(d, 3)) ? kV6Fused : kV6PairWide;
       }
     }
-    bn = (pl.variant == kV3Small || pl.variant == kV6Single || pl.variant == kV6Pair) ? 128 : 256;
+    bn = (pl.variant == kV3Small || pl.variant == kV6Single || pl.variant == kV6Pair || pl.variant == kV6Fused ||
+          pl.variant == kV3Fused)
+             ? 128
+             : 256;
+    pl.fused = pl.variant == kV3Fused || pl.variant == kV6Fused;
     pl.kpad = round_up(K, 8);
   }
   pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.variant == kV6PairC4 ||
-             pl.variant == kV6PairC2)
+             pl.variant == kV6PairC2 || pl.fused)
                 ? 1
                 : 0;
   pl.tile_m = pl.pair ? 256 : 128;
@@ -155,7 +182,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
   }
   const int es_in = pl.kind == 2 ? 1 : 2;
   const int es_out = pl.kind == 2 ? 8 : 4;
-  const size_t ls = (size_t)pl.layout_slices;
+  const size_t ls = pl.fused ? 0 : (size_t)pl.layout_slices;  // the fused kernel keeps no planes
   size_t off = 0;
   pl.off_b = off;
   off = al256(off + ls * N * pl.kpad * es_in);
@@ -186,6 +213,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di) {
 }
 
 static int plan_launches(const Plan& pl) {
+  if (pl.fused) return 1 + (pl.t.splits > 1 ? 1 : 0);
   if (pl.kind != 2) return 3 + (pl.t.splits > 1 ? 1 : 0);
   if (!pl.adaptive) return 4 + (pl.t.splits > 1 ? 1 : 0);
   // prep B (2), prep A, decision, the three gated kernels and their reductions
@@ -202,8 +230,10 @@ cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, cons
   return CUCOSMA_STATUS_SUCCESS;
 }
 
-void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info) {
-  const Plan pl = make_plan(d, di);
+bool tc_plan_is_fused(const cucosma_gemm_desc* d, const DeviceInfo* di) { return make_plan(d, di).fused != 0; }
+
+void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info, bool allow_fused) {
+  const Plan pl = make_plan(d, di, allow_fused);
   info->path = pl.kind + 1;
   info->tile_m = pl.tile_m;
   info->tile_n = pl.t.bn;
@@ -222,6 +252,7 @@ void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan
   info->off_part = pl.off_part;
   info->off_choice = pl.adaptive ? pl.off_stats + offsetof(OzakiStats, choice) : 0;
   info->layout_slices = pl.layout_slices;
+  info->fused = pl.fused;
 }
 
 cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
@@ -314,13 +345,35 @@ cudaError_t run_ozaki(const cucosma_gemm_desc* d, const Plan& pl, const Tiling& 
 
 cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
                           const DeviceInfo* di, cudaStream_t st, int prep) {
-  const Plan pl = make_plan(d, di);
+  // Callers that supply prepared planes (prep without both operands) never
+  // get the fused kernel, which reads the FP32 operands themselves.
+  const bool allow_fused = prep == (kPrepA | kPrepB) && A != nullptr && B != nullptr && d->flags == 0;
+  const Plan pl = make_plan(d, di, allow_fused);
   if (pl.kind == 2 && (pl.t.slices < 4 || pl.t.slices > 9)) return CUCOSMA_STATUS_NOT_SUPPORTED;
   uint8_t* w = static_cast<uint8_t*>(ws);
   const int m = (int)d->m, n = (int)d->n, k = (int)d->k;
   cudaError_t e = cudaSuccess;
   int launches = 0;
-  if (pl.kind != 2) {
+  if (pl.fused) {
+    // FP32 operand tiles straight from the caller's buffers: A [rows][32 K]
+    // boxes (128-byte swizzle), B [32 K][columns] boxes (row-major).
+    CUtensorMap ta, tb;
+    if (!encode_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, d->lda, 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, d->ldb, pl.bn_local, 32,
+                   CU_TENSOR_MAP_SWIZZLE_NONE))
+      return CUCOSMA_STATUS_LAUNCH_FAILED;
+    const TcParams p = tc_params(d, pl.t, pl, C, w, di);
+    prof_begin(st);
+    e = pl.kind == 1 ? launch_fused<Bf16x6Pair>(ta, tb, p, di->sms, st)
+                     : launch_fused<Bf16x3Pair128>(ta, tb, p, di->sms, st);
+    prof_end(st);
+    launches += 1;
+    if (e == cudaSuccess && pl.t.splits > 1) {
+      e = simt::launch_reduce<float>((const float*)p.out, p.ws_split_stride, pl.ldw, pl.t.splits, (float*)C, d->ldc, m,
+                                     n, d->alpha, d->beta, d->epilogue, di->sms, st);
+      launches += 1;
+    }
+  } else if (pl.kind != 2) {
     const int nt = pl.t.slices;
     if (prep & kPrepA) {
       e = launch_split_bf16((const float*)A, d->lda, m, k, pl.kpad, nt, w + pl.off_a, false, di->sms, st);

@@ -820,13 +820,17 @@ struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChu
 
 // CTA-pair tiles (256 rows): half the shared-memory operand reads and L2
 // traffic per output of the 128-row tiles at the same MMA N.
-//   Bf16x3Pair  256 x 256, one accumulator promoted every kPromoteChunk k-blocks.
+//   Bf16x3Pair  256 x 256, one accumulator promoted every kPromoteChunk k-blocks
+//               (Bf16x3Pair128: the 256 x 128 form, used with the fused split).
 //   Bf16x6Pair  256 x 128, main and correction accumulators (as Bf16x6),
 //               double-buffered.
 //   Bf16x6PairWide 256 x 256, main and correction accumulators filling TMEM
 //               (one buffer, split release); the 256 x 128 tiles need about
 //               1.5x the L2-to-shared-memory bandwidth per flop.
 struct Bf16x3Pair : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8, 0, true> {
+  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
+};
+struct Bf16x3Pair128 : TraitsBase<3, 128, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8, 0, true> {
   static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
 };
 struct Bf16x6Pair : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChunk, 8, 0, true> {

@@ -82,9 +82,13 @@ typedef struct cucosma_gemm_desc {
                            * NATIVE 1 = always the 128 x 128 tile kernel (no skinny-shape kernels),
                            *        2 = the 64 x 128 tile kernel (FP32; FP64 runs 128 x 128);
                            * BF16X3 1 = 128 x 256 without promotion, 2 = 128 x 128 promoted,
-                           *        3 = 128 x 256 promoted, 4 = 256 x 256 CTA pair (default when m > 128);
+                           *        3 = 128 x 256 promoted, 4 = 256 x 256 CTA pair (default when m > 128),
+                           *        5 = 256 x 128 pair with the split fused in;
                            * BF16X6 1 = 128 x 128, 2 = 256 x 128 CTA pair,
-                           *        3 = 256 x 256 CTA pair (default when m > 128) */
+                           *        3 = 256 x 256 CTA pair (default when m > 128),
+                           *        4 = 256 x 128 pair with the split fused in.
+                           * Auto (0) picks the fused kernels where the separate split pass
+                           * would cost more than a quarter of the GEMM (large K, large N) */
   int32_t flags;          /* 0, or CUCOSMA_FLAG_TEST_SKIP_STAGE */
 } cucosma_gemm_desc;
 
@@ -124,7 +128,8 @@ typedef struct cucosma_plan_info {
    * FP64.  0 for every other path. */
   uint64_t off_choice;
   int32_t layout_slices; /* Ozaki: slices per 32-wide k-block in the workspace layout */
-  int32_t reserved;
+  int32_t fused;         /* BF16 paths: 1 = the split is done inside the GEMM kernel (operands read once
+                          * from the caller's buffers; no planes in the workspace) */
 } cucosma_plan_info;
 CUCOSMA_API cucosma_status cucosma_gemm_get_plan(const cucosma_gemm_desc* d, cucosma_plan_info* info);
 

@@ -358,3 +358,55 @@ def test_ozaki_choice_matches_host_restatement():
             A, B = expspread(seed, (m, k), sigma=sigma), expspread(seed + 100, (k, n), sigma=sigma)
         _, plan, ws = run(A, B, np.zeros((m, n)), 1.0, 0.0, "ozaki", keep_ws=True)
         assert _choice(ws, plan) == oracle.ozaki_choice(A, B), (seed, sigma)
+
+
+# ---------------------------------------------------- split fused into the GEMM
+
+FUSED = [("bf16x3", 5, 4), ("bf16x6", 4, 2)]  # (precision, fused tile id, unfused tile id with the same arithmetic)
+FUSED_SHAPES = [(7, 5, 3), (129, 257, 33), (300, 200, 100), (513, 300, 700), (256, 256, 70000), (256, 5000, 256),
+                (700, 129, 1500)]
+
+
+@pytest.mark.parametrize("precision,ftile,utile", FUSED, ids=["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("shape", FUSED_SHAPES, ids=["%dx%dx%d" % s for s in FUSED_SHAPES])
+def test_fused_split_bitexact_vs_prepass(precision, ftile, utile, shape):
+    """The kernel that cuts the BF16 planes from FP32 tiles in shared memory
+    gives the same result bit for bit as the pre-pass + GEMM with the same
+    tile and promotion (alpha 1.5, beta 0.5, sigmoid), and stays inside the
+    split's bound against the FP64 oracle."""
+    m, n, k = shape
+    A = uniform(80, (m, k), lo=-0.5, hi=0.5)
+    B = uniform(81, (k, n), lo=-0.5, hi=0.5)
+    Cin = uniform(82, (m, n))
+    outf, planf = run(A, B, Cin, 1.5, 0.5, precision, epilogue="sigmoid", tile=ftile)
+    outu, planu = run(A, B, Cin, 1.5, 0.5, precision, epilogue="sigmoid", tile=utile)
+    assert planf["fused"] == 1 and planu["fused"] == 0
+    assert planf["launches"] == (2 if planf["splits"] > 1 else 1)
+    assert np.array_equal(outf, outu), (planf, planu)
+    _, b = bf16_bound(A, B, Cin, 1.5, 0.5, 2 if precision == "bf16x3" else 3)
+    ref = oracle.gemm(A, B, Cin, 1.5, 0.5, oracle.EPI_SIGMOID)
+    assert np.all(np.abs(outf - ref) <= 0.25 * b + 8 * 2.0 ** -24)
+
+
+@pytest.mark.parametrize("precision,ftile,utile", FUSED, ids=["bf16x3", "bf16x6"])
+def test_fused_split_forced_split_k(precision, ftile, utile):
+    A = uniform(83, (300, 9000))
+    B = uniform(84, (9000, 260))
+    Cin = uniform(85, (300, 260))
+    outf, planf = run(A, B, Cin, 1.0, -0.5, precision, split_k=5, tile=ftile)
+    outu, _ = run(A, B, Cin, 1.0, -0.5, precision, split_k=5, tile=utile)
+    assert planf["splits"] == 5 and np.array_equal(outf, outu)
+
+
+def test_fused_split_chosen_for_large_k():
+    """Auto planning picks the fused kernel where the operands are read about
+    once (256 x 256 x 262144) and not for a square problem."""
+    import torch
+
+    for prec in ("bf16x3", "bf16x6"):
+        A = torch.empty((256, 262144), device="cuda")
+        B = torch.empty((262144, 256), device="cuda")
+        Cm = torch.empty((256, 256), device="cuda")
+        assert cc.get_plan(cc.make_desc(A, B, Cm, precision=prec))["fused"] == 1
+        S = torch.empty((4096, 4096), device="cuda")
+        assert cc.get_plan(cc.make_desc(S, S, S, precision=prec))["fused"] == 0
