@@ -10,7 +10,7 @@ import pytest
 
 import cucosma_b200 as cc
 import oracle
-from tests._util import check_against_oracle, to_dev, uniform
+from tests._util import bound, check_against_oracle, to_dev, uniform
 
 pytestmark = pytest.mark.gpu
 
@@ -221,7 +221,10 @@ REF_TAGS = [t for t in oracle.ref_kernel_tags() if "8192" not in t]
 @pytest.mark.parametrize("tag", REF_TAGS)
 def test_parity_with_reference_kernel(cuda, tag):
     """Same seeded inputs through the reference kernel (compiled unmodified for
-    sm_100a) and through this library: both inside the FP64-oracle bound."""
+    sm_100a) and through this library: both inside the FP64-oracle bound, and
+    their difference from each other stated and bounded -- entrywise by the
+    sum of the two bounds (each is within its bound of the oracle), and
+    normwise by twice the larger of their two normwise errors plus u."""
     import torch
 
     ref = oracle.RefKernel(tag)
@@ -241,4 +244,12 @@ def test_parity_with_reference_kernel(cuda, tag):
     out = run(A, B, Cin, ref.alpha, ref.beta, dtype)
     e_ref = check_against_oracle(out_ref, A, B, Cin, ref.alpha, ref.beta, oracle.EPI_NONE, dtype)
     e_own = check_against_oracle(out, A, B, Cin, ref.alpha, ref.beta, oracle.EPI_NONE, dtype)
-    print(tag, "reference", e_ref, "cucosma", e_own)
+    # ours against the reference's own result on the same inputs
+    e_pair = oracle.errors(out, out_ref.astype(np.float64))
+    pre = oracle.gemm(A, B, Cin, ref.alpha, ref.beta)
+    b = bound(A, B, Cin, ref.alpha, ref.beta, oracle.EPI_NONE, dtype, pre)
+    diff = np.abs(out.astype(np.float64) - out_ref.astype(np.float64))
+    u = 2.0 ** -24 if dtype == np.float32 else 2.0 ** -53
+    print(tag, "reference", e_ref, "cucosma", e_own, "cucosma vs reference", e_pair)
+    assert np.all(diff <= 2 * b)
+    assert e_pair["normwise"] <= 2 * max(e_ref["normwise"], e_own["normwise"]) + u
