@@ -42,8 +42,6 @@ enum Variant : int {
   kV6Pair = 5,       // BF16x6 256 x 128 CTA pair, two double-buffered accumulators (tile id 2)
   kV6PairWide = 6,   // BF16x6 256 x 256 CTA pair, two accumulators, split release (tile id 3)
   kVOzaki = 7,
-  kV6PairC4 = 8,     // BF16x6 256 x 256 pair promoted every 4 k-blocks (tile id 5)
-  kV6PairC2 = 9,     // BF16x6 256 x 256 pair promoted every 2 k-blocks (tile id 6)
   kV3Fused = 10,     // BF16x3 256 x 128 pair, split fused into the kernel (tile id 5)
   kV6Fused = 11,     // BF16x6 256 x 128 pair, split fused into the kernel (tile id 4)
 };
@@ -105,15 +103,20 @@ static Tiling make_tiling(const Plan& pl, int slices, int bn, const cucosma_gemm
 // The fused split pays off when the separate pre-pass (read the FP32
 // operands, write nt BF16 planes) would take more than a quarter of the
 // GEMM's own bound (tensor time at nt products of BF16, or the HBM time of
-// reading the planes and writing -- with beta, also reading -- C): operands
-// read only a few times, as in the large-K and large-N families.
+// reading the planes and writing -- with beta, also reading -- C), and the
+// C traffic is small beside the operands' (the converter warps also run the
+// epilogue, so a C-heavy shape such as 256 x 1,048,576 x 256 would serialise
+// its stores with the next tile's conversion): operands read only a few
+// times with a small output, as in the large-K family.
 static bool fused_pays(const cucosma_gemm_desc* d, int nt) {
   const double M = (double)d->m, N = (double)d->n, K = (double)d->k;
   const double hbm = 6.5e12, bf16 = 1.6e15;
   const double products = nt == 2 ? 3.0 : 6.0;
+  const double c_bytes = M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0), ab_bytes = (M * K + K * N) * 4.0;
+  if (c_bytes > 0.25 * ab_bytes) return false;
   const double t_pre = (M * K + K * N) * (4.0 + 2.0 * nt) / hbm;
   const double t_mma = 2.0 * M * N * K * products / bf16;
-  const double t_mem = ((M * K + K * N) * 2.0 * nt + M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0)) / hbm;
+  const double t_mem = ((M * K + K * N) * 2.0 * nt + c_bytes) / hbm;
   return t_pre > 0.25 * std::max(t_mma, t_mem);
 }
 
@@ -152,8 +155,6 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool all
         case 2: pl.variant = kV6Pair; break;
         case 3: pl.variant = kV6PairWide; break;
         case 4: pl.variant = allow_fused ? kV6Fused : kV6Pair; break;
-        case 5: pl.variant = kV6PairC4; break;
-        case 6: pl.variant = kV6PairC2; break;
         default:
           pl.variant = !pair_ok ? kV6Single : (allow_fused && fused_pays(d, 3)) ? kV6Fused : kV6PairWide;
       }
@@ -165,10 +166,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool all
     pl.fused = pl.variant == kV3Fused || pl.variant == kV6Fused;
     pl.kpad = round_up(K, 8);
   }
-  pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.variant == kV6PairC4 ||
-             pl.variant == kV6PairC2 || pl.fused)
-                ? 1
-                : 0;
+  pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.fused) ? 1 : 0;
   pl.tile_m = pl.pair ? 256 : 128;
   pl.bn_local = pl.pair ? bn / 2 : bn;
   pl.t = make_tiling(pl, slices, bn, d, di);
@@ -400,12 +398,6 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
       case kV6Pair: e = launch<Bf16x6Pair>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6Pair>(di->sms)), st); break;
       case kV6PairWide:
         e = launch<Bf16x6PairWide>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWide>(di->sms)), st);
-        break;
-      case kV6PairC4:
-        e = launch<Bf16x6PairWideC<4>>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWideC<4>>(di->sms)), st);
-        break;
-      case kV6PairC2:
-        e = launch<Bf16x6PairWideC<2>>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x6PairWideC<2>>(di->sms)), st);
         break;
       case kV3Small: e = launch<Bf16x3Promoted>(ta, tb, p, grid, st); break;
       case kV3Wide: e = launch<Bf16x3Wide>(ta, tb, p, grid, st); break;

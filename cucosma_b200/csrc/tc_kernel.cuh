@@ -842,14 +842,6 @@ struct Bf16x6PairWide : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, kPr
       {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
 };
 
-// The same tile promoted every CH k-blocks (a shorter chunk bounds how long
-// the tensor cores' truncating accumulation runs between promotions).
-template <int CH>
-struct Bf16x6PairWideC : TraitsBase<6, 256, 64, 3, 3, 2, false, EpiF32, true, CH, 8, 0, true, true> {
-  static constexpr TermTable<6> kTerms{
-      {2, 1, 1, 0, 0, 0}, {0, 1, 0, 2, 1, 0}, {1, 1, 1, 1, 1, 0}, {true, false, false, false, false, true}};
-};
-
 // Ozaki with S slices: all pairs (p, q) with p + q < S, accumulated into
 // diagonal d = p + q.  Stacked form: S MMAs per sub-tile and k-block (one
 // per A slice, N shrinking with p) instead of S(S+1)/2 narrow ones -- an MMA

@@ -52,7 +52,9 @@ def test_split_planes_bitexact(precision, nterms):
     A = uniform(1, (m, k))
     B = uniform(2, (k, n))
     Cin = np.zeros((m, n), np.float32)
-    _, plan, ws = run(A, B, Cin, 1.0, 0.0, precision, keep_ws=True)
+    # a tile that runs the split pre-pass (the fused-split kernel keeps no planes)
+    _, plan, ws = run(A, B, Cin, 1.0, 0.0, precision, keep_ws=True, tile=3 if precision == "bf16x3" else 1)
+    assert plan["fused"] == 0
     kpad = plan["kpad"]
     raw = ws.view(np.uint16)
     pa = raw[plan["off_a"] // 2: plan["off_a"] // 2 + nterms * m * kpad].reshape(nterms, m, kpad)[:, :, :k]
