@@ -66,13 +66,18 @@ extern "C" cucosma_status cucosma_gemm_backward_workspace_size(const cucosma_gem
   if (!bytes) return CUCOSMA_STATUS_INVALID_VALUE;
   cucosma_status s = check_bwd(f);
   if (s != CUCOSMA_STATUS_SUCCESS) return s;
-  cucosma_gemm_desc da, db;
-  sub_desc(f, f->m, f->k, f->n, f->k, &da);
-  sub_desc(f, f->k, f->n, f->m, f->n, &db);
-  size_t a = 0, b = 0;
-  if ((s = cucosma_gemm_workspace_size(&da, &a)) != CUCOSMA_STATUS_SUCCESS) return s;
-  if ((s = cucosma_gemm_workspace_size(&db, &b)) != CUCOSMA_STATUS_SUCCESS) return s;
-  *bytes = std::max(a, b);
+  const DeviceInfo* di = device_info();
+  if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+  // Each product's plan as the backward call builds it: tuned, and with its
+  // planes prepared here (never the fused-split kernel, which keeps none).
+  auto need = [&](int64_t m, int64_t n, int64_t k, int64_t ldc) {
+    cucosma_gemm_desc d0, tuned;
+    cucosma_plan_info pi;
+    sub_desc(f, m, n, k, ldc, &d0);
+    tc_plan_info(apply_tuning(&d0, &tuned, di), di, &pi, false);
+    return pi.workspace_bytes;
+  };
+  *bytes = std::max(need(f->m, f->k, f->n, f->k), need(f->k, f->n, f->m, f->n));
   return CUCOSMA_STATUS_SUCCESS;
 }
 

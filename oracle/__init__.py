@@ -176,7 +176,7 @@ def ozaki_gemm(A, B, s, Cin=None, alpha=1.0, beta=0.0, epilogue=EPI_NONE, kchunk
 
 
 def errors(x, ref, ref_lo=None):
-    """max / mean elementwise relative error and normwise error of x vs ref.
+    """max / mean / median elementwise relative error and normwise error of x vs ref.
 
     Elementwise relative error uses max(|ref|, tiny) so exact zeros do not
     divide by zero; normwise = ||x - ref||_F / ||ref||_F."""
@@ -192,6 +192,7 @@ def errors(x, ref, ref_lo=None):
     return {
         "max_rel": float(rel.max()) if rel.size else 0.0,
         "mean_rel": float(rel.mean()) if rel.size else 0.0,
+        "median_rel": float(np.median(rel)) if rel.size else 0.0,
         "normwise": float(np.linalg.norm(d) / nrm) if nrm > 0 else float(np.linalg.norm(d)),
         "max_abs": float(np.abs(d).max()) if d.size else 0.0,
     }
