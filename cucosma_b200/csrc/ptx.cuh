@@ -74,12 +74,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase with the given parity to complete.
+// Acquire at cluster scope: for a barrier that threads of the other CTA of
+// a pair arrive on (their release is at cluster scope too).
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+template <bool CLUSTER = false>
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int err_code, const WaitCtl& ctl) {
   const uint32_t a = smem_u32(bar);
-  if (mbar_try_wait(a, parity)) return true;
+  auto poll = [&]() { return CLUSTER ? mbar_try_wait_cluster(a, parity) : mbar_try_wait(a, parity); };
+  if (poll()) return true;
   const uint64_t t0 = globaltimer();
   while (true) {
-    if (mbar_try_wait(a, parity)) return true;
+    if (poll()) return true;
     if (globaltimer() - t0 > ctl.timeout_ns) {
       record_error(ctl, err_code);
       return false;

@@ -30,6 +30,23 @@ __device__ __forceinline__ void split_bf16_n(float x, __nv_bfloat16 (&t)[NT]) {
   }
 }
 
+// Two values at once: w[i] holds term i of x0 in its low half and of x1 in
+// its high half (cvt.rn.bf16x2.f32 rounds each to nearest even, as
+// __float2bfloat16_rn does), so the words equal pack_bf16x2 of
+// split_bf16_n's terms bit for bit.
+template <int NT>
+__device__ __forceinline__ void split_bf16x2_n(float x0, float x1, uint32_t (&w)[NT]) {
+  float r0 = x0, r1 = x1;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w[i]) : "f"(r1), "f"(r0));
+    if (i + 1 < NT) {
+      r0 = r0 - __uint_as_float(w[i] << 16);
+      r1 = r1 - __uint_as_float(w[i] & 0xffff0000u);
+    }
+  }
+}
+
 __device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
   __nv_bfloat162 v = __halves2bfloat162(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);

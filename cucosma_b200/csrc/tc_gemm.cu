@@ -353,17 +353,21 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
   cudaError_t e = cudaSuccess;
   int launches = 0;
   if (pl.fused) {
-    // FP32 operand tiles straight from the caller's buffers: A [rows][32 K]
-    // boxes (128-byte swizzle), B [32 K][columns] boxes (row-major).
+    // FP32 operand tiles straight from the caller's buffers.  BF16x3 (in
+    // place): A [128 rows][64 K] and B [64 K][64 columns] boxes, 256-byte
+    // rows; BF16x6: A [128 rows][32 K] (128-byte swizzle) and B [32 K][64].
+    const bool inplace = pl.kind == 0;
+    const int kw = inplace ? 64 : 32;
     CUtensorMap ta, tb;
-    if (!encode_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, d->lda, 32, 128, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !encode_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, d->ldb, pl.bn_local, 32,
+    if (!encode_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, d->lda, kw, 128,
+                   inplace ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, d->ldb, pl.bn_local, kw,
                    CU_TENSOR_MAP_SWIZZLE_NONE))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     const TcParams p = tc_params(d, pl.t, pl, C, w, di);
     prof_begin(st);
-    e = pl.kind == 1 ? launch_fused<Bf16x6Pair>(ta, tb, p, di->sms, st)
-                     : launch_fused<Bf16x3Pair128>(ta, tb, p, di->sms, st);
+    e = inplace ? launch_fused_inplace<Bf16x3Pair128>(ta, tb, p, di->sms, st)
+                : launch_fused<Bf16x6Pair>(ta, tb, p, di->sms, st);
     prof_end(st);
     launches += 1;
     if (e == cudaSuccess && pl.t.splits > 1) {

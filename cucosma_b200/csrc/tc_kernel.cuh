@@ -361,7 +361,7 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
         for (int cs = u.kb0; cs < kb1 && ok; cs += chunk, ++ci) {
           const int ce = min(kb1, cs + chunk);
           const int buf = ci % NBUF;
-          if (!Tr::SPLIT && !mbar_wait(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+          if (!Tr::SPLIT && !mbar_wait<PAIR>(&tempty[buf], ((ci / NBUF) & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
             ok = false;
             break;
           }
@@ -380,13 +380,13 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
               // corrections (terms 0 .. NT-2, accumulator 1) once that
               // accumulator is drained, then the main term (accumulator 0)
               const uint64_t bd0 = sdesc<SWZ>(a_base + A_REGION);
-              if (kb == cs && !mbar_wait(&tempty[1], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+              if (kb == cs && !mbar_wait<PAIR>(&tempty[1], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
                 ok = false;
                 break;
               }
               tc_fence_after();
               issue_terms<Tr>(std::make_integer_sequence<int, Tr::NT - 1>{}, ad0, bd0, acc0, kb != cs);
-              if (kb == cs && !mbar_wait(&tempty[0], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
+              if (kb == cs && !mbar_wait<PAIR>(&tempty[0], (ci & 1) ^ 1, kErrTimeoutAccumFree, p.ctl)) {
                 ok = false;
                 break;
               }
