@@ -38,16 +38,38 @@ enum Epilogue : int { kEpiNone = 0, kEpiSigmoid = 1, kEpiRelu = 2 };
 
 // Fused activation applied to the final value (cuCOSMAV100.cuh:2466-2476
 // holds the reference's ReLU / Sigmoid loops; sigmoid4.cuh:19-22 the formula).
+// epi_t<EPI>: the activation fixed at compile time, for epilogues that
+// dispatch once per block.
+template <int EPI>
+__device__ __forceinline__ float epi_t(float v) {
+  if constexpr (EPI == kEpiSigmoid) return 1.0f / (1.0f + expf(-v));
+  else if constexpr (EPI == kEpiRelu) return fmaxf(v, 0.0f);
+  else return v;
+}
+template <int EPI>
+__device__ __forceinline__ double epi_t(double v) {
+  if constexpr (EPI == kEpiSigmoid) return 1.0 / (1.0 + exp(-v));
+  else if constexpr (EPI == kEpiRelu) return fmax(v, 0.0);
+  else return v;
+}
+// apply_epi: chosen at run time per value.  The sigmoid is a call, never
+// inlined: inlined, the compiler if-converted it, evaluating the exponential
+// and the division for every element of every epilogue (that made the FP32
+// tensor-core epilogue five times slower on B200 with no activation at all).
+__device__ __noinline__ float sigmoid_f32(float v);
+__device__ __noinline__ double sigmoid_f64(double v);
 __device__ __forceinline__ float apply_epi(float v, int epi) {
-  if (epi == kEpiSigmoid) return 1.0f / (1.0f + expf(-v));
   if (epi == kEpiRelu) return fmaxf(v, 0.0f);
+  if (epi == kEpiSigmoid) return sigmoid_f32(v);
   return v;
 }
 __device__ __forceinline__ double apply_epi(double v, int epi) {
-  if (epi == kEpiSigmoid) return 1.0 / (1.0 + exp(-v));
   if (epi == kEpiRelu) return fmax(v, 0.0);
+  if (epi == kEpiSigmoid) return sigmoid_f64(v);
   return v;
 }
+__device__ __noinline__ inline float sigmoid_f32(float v) { return epi_t<kEpiSigmoid>(v); }
+__device__ __noinline__ inline double sigmoid_f64(double v) { return epi_t<kEpiSigmoid>(v); }
 
 // alpha/beta combination.  The reference scales the accumulator by ALPHA
 // first and then adds BETA*C (cuCOSMAV100.cuh:1582-1593, :901); written here

@@ -27,6 +27,7 @@ enum DeviceError : int {
   kErrTimeoutAccum = 0x103,     // epilogue gave up waiting for an accumulator
   kErrTimeoutAccumFree = 0x104, // MMA warp gave up waiting for a drained accumulator
   kErrTimeoutDrain = 0x105,     // exit path gave up waiting for its own copies
+  kErrTimeoutOutput = 0x106,    // epilogue gave up waiting for its C tile
   kErrBadTmem = 0x201,          // TMEM allocation returned an unusable address
 };
 
@@ -129,6 +130,56 @@ __device__ __forceinline__ void tma_load_3d(void* smem_dst, const CUtensorMap* m
           smem_u32(smem_dst)),
       "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
+}
+
+// L2 prefetch of one tensor-map box (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* m, int32_t x, int32_t y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(m)),
+               "r"(x), "r"(y)
+               : "memory");
+}
+// Tiled store shared -> global (completion tracked by bulk groups): the
+// commit, and the waits for the smem reads of all groups / for all groups to
+// finish writing.  Out-of-range rows and columns of the box are not written.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* m, const void* smem_src, int32_t x, int32_t y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(m)),
+               "r"(smem_u32(smem_src)), "r"(x), "r"(y)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Arrive-with-transaction returning the phase token, and the bounded wait
+// for that phase (no parity bookkeeping for a barrier one thread reuses).
+__device__ __forceinline__ uint64_t mbar_arrive_expect_tx_token(uint64_t* bar, uint32_t bytes) {
+  uint64_t t;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;" : "=l"(t) : "r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  return t;
+}
+__device__ __forceinline__ bool mbar_try_wait_token(uint32_t bar, uint64_t token) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "l"(token)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_token(uint64_t* bar, uint64_t token, int err_code, const WaitCtl& ctl) {
+  const uint32_t a = smem_u32(bar);
+  if (mbar_try_wait_token(a, token)) return true;
+  const uint64_t t0 = globaltimer();
+  while (true) {
+    if (mbar_try_wait_token(a, token)) return true;
+    if (globaltimer() - t0 > ctl.timeout_ns) {
+      record_error(ctl, err_code);
+      return false;
+    }
+  }
 }
 
 // 4-byte asynchronous copy global -> shared (no register is written; many

@@ -131,7 +131,8 @@ __device__ __forceinline__ bool forward_planes(uint64_t* local_bar, uint32_t par
 
 template <class Tr, int G>
 __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
-    tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+    tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    const __grid_constant__ TcParams p) {
   using F = FusedCfg<Tr, G>;
   constexpr int BN = Tr::BN, NACC = Tr::NACC, PS = F::PS, RS = F::RS, NBUF = Tr::NBUF, TILE_M = Tr::TILE_M;
   constexpr int A_REGION = Tr::A_REGION;
@@ -149,7 +150,8 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
   uint64_t* tfull = raw_empty + RS;
   uint64_t* tempty = tfull + 4;
   uint64_t* drain = tempty + 4;
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* ebar = drain + 1;  // one per promotion/epilogue warp: its TMA loads of C
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + F::ACC_WARPS);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.tiles_m * p.tiles_n * p.splits;
@@ -171,6 +173,7 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
       mbar_init(&tempty[b], 2 * F::ACC_WARPS);
     }
     mbar_init(drain, 1);
+    for (int w = 0; w < F::ACC_WARPS; ++w) mbar_init(&ebar[w], 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -260,7 +263,14 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
       resolve_unit(p, &tmA, &tmB, unit, u);
       const int row0 = u.tm * TILE_M + (int)rank * 128 + 32 * q;
       const int col0 = u.tn * BN;
-      prefetch_c_block(out_ctx(p, u), row0, col0 + colsub, W, 4, lane);
+      // C prefetched into L2 one unit ahead (this unit's only for the first)
+      auto prefetch_unit = [&](int un) {
+        if (un >= units) return;
+        Unit v;
+        resolve_unit(p, &tmA, &tmB, un, v);
+        prefetch_c_block(out_ctx(p, v), v.tm * TILE_M + (int)rank * 128 + 32 * q, v.tn * BN + colsub, W, 4, lane);
+      };
+      if (unit == unit0) prefetch_unit(unit);
       const int nchunks = (u.kb1 - u.kb0 + chunk - 1) / chunk;
       float master[W];
 #pragma unroll
@@ -279,9 +289,13 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
         if (lane == 0) mbar_arrive_cluster(tempty_rank0 + (uint32_t)(buf * sizeof(uint64_t)));
       }
       if (!ok) break;
-      Tr::finish(out_ctx(p, u), master, stg, lane, row0, col0 + colsub, u.z);
+      prefetch_unit(unit + unit_step);
+      OutCtx o = out_ctx(p, u);
+      o.tbar = &ebar[warp - 2];
+      Tr::finish(o, master, stg, lane, row0, col0 + colsub, u.z);
       ci += nchunks;
     }
+    if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed
   } else {
     // --------------------------------------------------------- converters
     const int cw = warp - F::CONV_WARP0;  // 0..5: A warps 0-3, B warps 4-5
@@ -425,7 +439,7 @@ __device__ __forceinline__ bool inplace_convert_b(uint8_t* stage, int c, Sync&& 
 template <class Tr>
 __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
     tc_fused_inplace_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                            const TcParams p) {
+                            const __grid_constant__ TcParams p) {
   using F = FusedInplaceCfg<Tr>;
   constexpr int BN = Tr::BN, NACC = Tr::NACC, NS = F::NS, NBUF = Tr::NBUF, TILE_M = Tr::TILE_M;
   constexpr int A_REGION = Tr::A_REGION;
@@ -443,7 +457,8 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
   uint64_t* drain = tempty + 4;
   uint64_t* conv_rd = drain + 1;  // this CTA's converters have read the stage's FP32 values
   uint64_t* fwd = conv_rd + 1;    // rank 1: this CTA's converters wrote the stage (forwarded to rank 0)
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(fwd + NS);
+  uint64_t* ebar = fwd + NS;      // one per promotion/epilogue warp: its TMA loads of C
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + F::ACC_WARPS);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.tiles_m * p.tiles_n * p.splits;
@@ -464,6 +479,7 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
       mbar_init(&tempty[b], 2 * F::ACC_WARPS);
     }
     mbar_init(drain, 1);
+    for (int w = 0; w < F::ACC_WARPS; ++w) mbar_init(&ebar[w], 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -569,7 +585,14 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
       resolve_unit(p, &tmA, &tmB, unit, u);
       const int row0 = u.tm * TILE_M + (int)rank * 128 + 32 * q;
       const int col0 = u.tn * BN;
-      prefetch_c_block(out_ctx(p, u), row0, col0 + colsub, W, 4, lane);
+      // C prefetched into L2 one unit ahead (this unit's only for the first)
+      auto prefetch_unit = [&](int un) {
+        if (un >= units) return;
+        Unit v;
+        resolve_unit(p, &tmA, &tmB, un, v);
+        prefetch_c_block(out_ctx(p, v), v.tm * TILE_M + (int)rank * 128 + 32 * q, v.tn * BN + colsub, W, 4, lane);
+      };
+      if (unit == unit0) prefetch_unit(unit);
       const int nchunks = (u.kb1 - u.kb0 + chunk - 1) / chunk;
       float master[W];
 #pragma unroll
@@ -588,9 +611,13 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
         if (lane == 0) mbar_arrive_cluster(tempty_rank0 + (uint32_t)(buf * sizeof(uint64_t)));
       }
       if (!ok) break;
-      Tr::finish(out_ctx(p, u), master, stg, lane, row0, col0 + colsub, u.z);
+      prefetch_unit(unit + unit_step);
+      OutCtx o = out_ctx(p, u);
+      o.tbar = &ebar[warp - 2];
+      Tr::finish(o, master, stg, lane, row0, col0 + colsub, u.z);
       ci += nchunks;
     }
+    if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed
   } else {
     // --------------------------------------------------------- converters
     // conv_rd completes once per stage, in stage order (a warp arrives for

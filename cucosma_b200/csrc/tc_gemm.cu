@@ -3,6 +3,7 @@
 #include "simt_gemm.cuh"
 #include "split.cuh"
 #include "tc_fused.cuh"
+#include <cstdlib>
 #include "tc_kernel.cuh"
 
 namespace cucosma {
@@ -287,6 +288,21 @@ TcParams tc_params(const cucosma_gemm_desc* d, const Tiling& t, const Plan& pl, 
     p.partial = 0;
     p.out = C;
     p.ldo = d->ldc;
+    // FP32 results leave through TMA when C allows a tensor map (16-byte
+    // aligned base and rows) and its rows end on a 16-byte boundary (a box
+    // store clips the columns past N only to the 16-byte granule: on B200 it
+    // wrote the rest of the last granule); otherwise the epilogue stores rows
+    // itself.  CUCOSMA_TMA_EPILOGUE=0 turns the TMA path off.
+    static const bool tma_epilogue = [] {
+      const char* e = std::getenv("CUCOSMA_TMA_EPILOGUE");
+      return !(e && e[0] == '0');
+    }();
+    if (tma_epilogue && pl.kind != 2 && C != nullptr && (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
+        (d->ldc * 4) % 16 == 0 && d->n % 4 == 0)
+      p.tma_out = encode_2d(&p.tmc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)d->n, (uint64_t)d->m,
+                            (uint64_t)d->ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B)
+                      ? 1
+                      : 0;
   }
   return p;
 }

@@ -42,6 +42,11 @@ struct alignas(64) GroupEntry {
 };
 
 struct TcParams {
+  // FP32 output C through TMA (tma_out = 1): 32 x 32 boxes, 128-byte
+  // swizzle; used by the epilogue for whole-problem outputs (not split-K
+  // partials, not grouped launches).
+  CUtensorMap tmc;
+  int tma_out;
   int m, n, k;
   int tiles_m, tiles_n;
   int kblocks;       // k-blocks of the whole K
@@ -78,6 +83,9 @@ struct OutCtx {
   int64_t ldo, ws_split_stride;
   const int32_t* ea;
   const int32_t* eb;
+  const CUtensorMap* tmc;  // non-null: the FP32 epilogue moves C by TMA
+  uint64_t* tbar;          // this epilogue warp's barrier for its C loads
+  WaitCtl ctl;
 };
 
 // A resolved work unit: operand descriptors, tile coordinates, K range.

@@ -31,6 +31,7 @@
 // Every mbarrier wait is bounded (ptx.cuh); on expiry the roles leave their
 // loops, drain what they issued, and TMEM is released before exit.
 #pragma once
+#include <type_traits>
 #include <cuda_bf16.h>
 
 #include <utility>
@@ -108,6 +109,14 @@ __device__ __forceinline__ void resolve_unit(const TcParams& p, const CUtensorMa
 // last element).
 __device__ __forceinline__ void prefetch_c_block(const OutCtx& o, int row0, int col0, int cols, int es, int lane) {
   if (o.partial || o.beta == 0.0 || col0 >= o.n) return;
+  if (o.tmc != nullptr) {
+    // the TMA epilogue's boxes, prefetched by the async proxy (the
+    // epilogue's own proxy fences then have no prefetches of their own to
+    // wait for)
+    if (lane == 0)
+      for (int c = col0; c < col0 + cols && c < o.n; c += 32) tma_prefetch_2d(o.tmc, c, row0);
+    return;
+  }
   const int c1 = min(o.n, col0 + cols);
   const int lines = ((c1 - col0) * es + 127) / 128 + 1;  // rows need not start on a line
   const char* base = static_cast<const char*>(o.out);
@@ -126,6 +135,9 @@ __device__ __forceinline__ OutCtx out_ctx(const TcParams& p, const Unit& u) {
   o.epilogue = p.epilogue;
   o.alpha = p.alpha;
   o.beta = p.beta;
+  o.ctl = p.ctl;
+  o.tbar = nullptr;
+  o.tmc = (u.group < 0 && p.tma_out && !p.partial) ? &p.tmc : nullptr;
   if (u.group < 0) {
     o.m = p.m;
     o.n = p.n;
@@ -226,7 +238,8 @@ __device__ __forceinline__ void commit_self(uint64_t* bar) {
 // Register cap: what one CTA per SM can give each thread (see MAX_REGS).
 template <class Tr>
 __global__ void __maxnreg__(Tr::MAX_REGS)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ TcParams p) {
   constexpr int BN = Tr::BN, SWZ = Tr::SWZ, NA = Tr::NA, NB = Tr::NB, NACC = Tr::NACC, ST = Tr::STAGES;
   constexpr int A_REGION = Tr::A_REGION;
   constexpr int STAGE_BYTES = Tr::STAGE_BYTES;
@@ -248,8 +261,10 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
   uint64_t* tfull = bars + 2 * ST;
   uint64_t* tempty = tfull + 4;
   uint64_t* drain = tempty + 4;
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* ebar = drain + 1;  // one per epilogue warp: its TMA loads of C
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + Tr::EPI_WARPS);
   static_assert(NBUF <= 4, "accumulator buffers");
+  static_assert((2 * ST + 9 + Tr::EPI_WARPS) * 8 + 4 <= 512, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.ngroups > 0 ? p.total_tiles : p.tiles_m * p.tiles_n * p.splits;
@@ -273,6 +288,7 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
       mbar_init(&tempty[b], Tr::EPI_WARPS * (PAIR ? 2 : 1));  // rank 0's: released by both CTAs' epilogues
     }
     mbar_init(drain, 1);
+    for (int w = 0; w < Tr::EPI_WARPS; ++w) mbar_init(&ebar[w], 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -436,11 +452,25 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
     for (int unit = unit0; unit < units && ok; unit += unit_step) {
       Unit u;
       resolve_unit(p, &tmA, &tmB, unit, u);
-      const OutCtx o = out_ctx(p, u);
       const int z = u.z;
       const int row0 = u.tm * TILE_M + (int)rank * 128 + 32 * q;
       const int col0 = u.tn * BN;
-      prefetch_c_block(o, row0, col0 + (Tr::PROMOTE ? colsub : 0), Tr::PROMOTE ? W : BN, Tr::kInt8 ? 8 : 4, lane);
+      // C blocks are prefetched into L2 one unit ahead: this unit's (first
+      // unit only) and, before this unit's epilogue reads its C, the next's.
+      auto prefetch_unit = [&](int un) {
+        if (un >= units) return;
+        Unit v;
+        resolve_unit(p, &tmA, &tmB, un, v);
+        prefetch_c_block(out_ctx(p, v), v.tm * TILE_M + (int)rank * 128 + 32 * q,
+                         v.tn * BN + (Tr::PROMOTE ? colsub : 0), Tr::PROMOTE ? W : BN, Tr::kInt8 ? 8 : 4, lane);
+      };
+      if (unit == unit0) prefetch_unit(unit);
+      // the output context is built where it is used (fewer registers held across the chunk loop)
+      auto octx = [&]() {
+        OutCtx o = out_ctx(p, u);
+        o.tbar = &ebar[warp - 2];
+        return o;
+      };
       if constexpr (Tr::PROMOTE) {
         float master[W];
 #pragma unroll
@@ -462,17 +492,20 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
           }
         }
         if (!ok) break;
-        Tr::finish(o, master, stg, lane, row0, col0 + colsub, z);
+        prefetch_unit(unit + unit_step);
+        Tr::finish(octx(), master, stg, lane, row0, col0 + colsub, z);
       } else {
         const int buf = ci % NBUF;
         ok = __all_sync(0xffffffffu, mbar_wait(&tfull[buf], (ci / NBUF) & 1, kErrTimeoutAccum, p.ctl));
         if (!ok) break;
         tc_fence_after();
-        Tr::epilogue(o, lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
+        prefetch_unit(unit + unit_step);
+        Tr::epilogue(octx(), lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
         release(buf);
         ++ci;
       }
     }
+    if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed
   }
 
   tc_fence_before();
@@ -494,42 +527,102 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
 // FP32 result (BF16 split paths).  Each warp owns 32 rows; chunks of 32
 // columns go TMEM -> registers -> padded shared tile -> coalesced rows.
 struct EpiF32 {
-  static constexpr int STAGING_PER_WARP = 32 * 33 * 4;
+  // A 32 x 32 FP32 block per warp: row r's 16-byte chunk c at c ^ (r & 7)
+  // (the 128-byte swizzle TMA uses; the buffer is 1024-byte aligned).  Rows
+  // are read and written as float4 chunks by the lane owning the row, and
+  // columns one float per lane -- both free of bank conflicts.
+  static constexpr int STAGING_PER_WARP = 32 * 32 * 4;
+  static __device__ __forceinline__ int sw(int r, int c) { return r * 32 + ((((c >> 2) ^ (r & 7))) << 2) + (c & 3); }
 
-  // Writes one 32 x 32 block of results: acc[j] is this lane's row (row0 +
-  // lane) at column col + j.  With beta != 0 the C block is first copied into
-  // stg by cp.async (lanes = columns, all 32 rows in flight at once, so the
-  // block costs one memory latency; C was prefetched into L2), each lane
-  // combines its row from stg, and the results leave through stg as
-  // coalesced 128-byte row stores (lanes = columns).  Split-K partials are
-  // stored raw.  stg is a padded 32 x 33 tile (row r at r * 33), so both the
-  // row and the column accesses are free of bank conflicts.
+  // This lane's row of the block: epi(alpha * acc + beta * C) with C read
+  // from (and the result written back to) the swizzled staging row s4.
+  template <int EPI>
+  static __device__ __forceinline__ void combine_row_t(float4* s4, const float (&acc)[32], float alpha, float beta,
+                                                       int lane) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int pos = c ^ (lane & 7);
+      const float4 cv = beta != 0.f ? s4[pos] : make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 r;
+      r.x = epi_t<EPI>(combine(acc[4 * c], alpha, beta, &cv.x));
+      r.y = epi_t<EPI>(combine(acc[4 * c + 1], alpha, beta, &cv.y));
+      r.z = epi_t<EPI>(combine(acc[4 * c + 2], alpha, beta, &cv.z));
+      r.w = epi_t<EPI>(combine(acc[4 * c + 3], alpha, beta, &cv.w));
+      s4[pos] = r;
+    }
+  }
+  static __device__ __forceinline__ void combine_row(int epi, float4* s4, const float (&acc)[32], float alpha,
+                                                     float beta, int lane) {
+    if (epi == kEpiSigmoid)
+      combine_row_t<kEpiSigmoid>(s4, acc, alpha, beta, lane);
+    else if (epi == kEpiRelu)
+      combine_row_t<kEpiRelu>(s4, acc, alpha, beta, lane);
+    else
+      combine_row_t<kEpiNone>(s4, acc, alpha, beta, lane);
+  }
+
+  // Write one 32 x 32 block of results: acc[j] is this lane's row (row0 +
+  // lane) at column col + j.
+  //  * store_block_tma (p.tmc set): lane 0 waits until the previous block's store has read
+  //    the buffer, brings the C block in (beta != 0; out-of-range rows and
+  //    columns read as zero), every lane combines its row in place, and lane
+  //    0 stores the block (out-of-range parts are not written) -- a handful
+  //    of instructions per element, no predicates, C moved as whole boxes.
+  //  * store_block (split-K partials, grouped problems, unaligned C): C is
+  //    fetched by cp.async (lanes = columns, all rows in flight; C was
+  //    prefetched into L2), combined per row, and stored as 128-byte rows;
+  //    partials are stored raw.
+  static __device__ __forceinline__ void store_block_tma(const OutCtx& p, const float (&acc)[32], float* stg, int lane,
+                                                         int row0, int col) {
+    if (col >= p.n) return;  // the whole block lies right of C (col is the block's first column)
+    const float alpha = (float)p.alpha, beta = (float)p.beta;
+    float4* s4 = reinterpret_cast<float4*>(stg) + lane * 8;  // this lane's row
+    {
+      if (lane == 0) bulk_wait_read_all();
+      __syncwarp();
+      if (beta != 0.f) {
+        if (lane == 0) {
+          const uint64_t token = mbar_arrive_expect_tx_token(p.tbar, 32 * 32 * 4);
+          tma_load_2d(stg, p.tmc, col, row0, p.tbar);
+          if (!mbar_wait_token(p.tbar, token, kErrTimeoutOutput, p.ctl))
+            mbar_wait_token(p.tbar, token, kErrTimeoutDrain, p.ctl);  // once more before the buffer is reused
+        }
+        __syncwarp();
+      }
+      combine_row(p.epilogue, s4, acc, alpha, beta, lane);
+      fence_proxy_async_smem();  // the block is read by TMA (async proxy)
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(p.tmc, stg, col, row0);
+        bulk_commit();
+      }
+    }
+  }
+
   static __device__ __forceinline__ void store_block(const OutCtx& p, float* o, const float (&acc)[32], float* stg,
                                                      int lane, int row0, int col) {
     if (col >= p.n) return;  // the whole block lies right of C (col is the block's first column)
+    const float alpha = (float)p.alpha, beta = (float)p.beta;
+    float4* s4 = reinterpret_cast<float4*>(stg) + lane * 8;  // this lane's row
     const int cl = col + lane;  // this lane's column in the store pass
     if (p.partial) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = acc[j];
+      for (int c = 0; c < 8; ++c)
+        s4[c ^ (lane & 7)] = make_float4(acc[4 * c], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
     } else {
-      const float alpha = (float)p.alpha, beta = (float)p.beta;
       if (beta != 0.f) {
 #pragma unroll 4
         for (int r = 0; r < 32; ++r) {
           const int row = row0 + r;
           if (row < p.m && cl < p.n)
-            cp_async4(&stg[r * 33 + lane], o + (int64_t)row * p.ldo + cl);
+            cp_async4(&stg[sw(r, lane)], o + (int64_t)row * p.ldo + cl);
           else
-            stg[r * 33 + lane] = 0.f;
+            stg[sw(r, lane)] = 0.f;
         }
         cp_async_wait_all();
         __syncwarp();
       }
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const float c = beta != 0.f ? stg[lane * 33 + j] : 0.f;
-        stg[lane * 33 + j] = apply_epi(combine(acc[j], alpha, beta, &c), p.epilogue);
-      }
+      combine_row(p.epilogue, s4, acc, alpha, beta, lane);
     }
     __syncwarp();
     if (cl < p.n) {
@@ -538,7 +631,7 @@ struct EpiF32 {
 #pragma unroll 4
       for (int r = 0; r < 32; ++r) {
         const int row = row0 + r;
-        if (row < p.m) w[(int64_t)row * ld] = stg[r * 33 + lane];
+        if (row < p.m) w[(int64_t)row * ld] = stg[sw(r, lane)];
       }
     }
     __syncwarp();
@@ -561,7 +654,10 @@ struct EpiF32 {
         acc[j] = __uint_as_float(v0[j]);
         acc[16 + j] = __uint_as_float(v1[j]);
       }
-      store_block(p, o, acc, stg, lane, row0, col0 + c0);
+      if (p.tmc != nullptr)
+        store_block_tma(p, acc, stg, lane, row0, col0 + c0);
+      else
+        store_block(p, o, acc, stg, lane, row0, col0 + c0);
     }
   }
 
@@ -606,6 +702,16 @@ struct EpiF32 {
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[BN], uint8_t* stg_raw,
                                                 int lane, int row0, int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
+    if (p.tmc != nullptr) {
+#pragma unroll
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        float acc[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] = master[c0 + j];
+        store_block_tma(p, acc, stg, lane, row0, col0 + c0);
+      }
+      return;
+    }
     float* o = reinterpret_cast<float*>(p.out) + (p.partial ? (int64_t)z * p.ws_split_stride : 0);
 #pragma unroll
     for (int c0 = 0; c0 < BN; c0 += 32) {
@@ -749,13 +855,15 @@ struct TraitsBase {
                              B_SUB_BYTES % 256 == 0 && NACC_ == NB_),
                 "stacked form: INT8, whole sub-tiles, MMA N <= 256");
   static_assert(!PAIR_ || (!PACKED && BN_ % 32 == 0 && BN_ <= 256), "pair tiles: BF16 planes, MMA N <= 256");
-  static constexpr int FIXED = 1024 + STAGING_BYTES + 256;
+  static constexpr int FIXED = 1024 + STAGING_BYTES + 512;
   static constexpr int STAGES_FIT = (kSmemBudget - FIXED) / STAGE_BYTES;
   static constexpr int STAGES = STAGES_FIT > 6 ? 6 : STAGES_FIT;
   static constexpr int SMEM = FIXED + STAGES * STAGE_BYTES;
   static_assert(STAGES >= 2, "at least a double-buffered ring");
   static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
   static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
+  static_assert(!std::is_same<Epi, EpiF32>::value || STAGE_BYTES % 1024 == 0,
+                "the FP32 epilogue's swizzled staging starts 1024-byte aligned");
   static_assert(!PROMOTE || (CHUNK > 0 && (NBUF >= 2 || SPLIT_)), "promotion needs chunk buffers");
   static_assert(!SPLIT_ || (PROMOTE_ && NACC_ == 2 && NBUF == 1), "split release: two accumulators, one buffer");
   static __device__ __forceinline__ void epilogue(const OutCtx& p, uint32_t tacc, uint8_t* stg, int lane, int row0,

@@ -24,6 +24,9 @@ CASES = [  # (precision, dtype, m, n, k, split_k[, tile])
     ("bf16x6", np.float32, 130, 70, 45, 0), ("ozaki", np.float64, 129, 65, 33, 0),
     ("ozaki", np.float64, 70, 90, 3000, 3),
     ("native", np.float32, 130, 67, 45, 0, 2), ("native", np.float32, 65, 300, 3000, 3, 2),
+    # N a multiple of 4: C leaves through TMA boxes (partial tiles right and below)
+    ("bf16x3", np.float32, 129, 260, 65, 0), ("bf16x6", np.float32, 130, 72, 45, 0),
+    ("bf16x3", np.float32, 300, 132, 3000, 0, 5), ("bf16x6", np.float32, 300, 132, 3000, 0, 4),
 ]
 
 
