@@ -57,7 +57,9 @@ struct FusedCfg {
   // room for five raw stages (a stage is refilled as soon as the MMAs that
   // read it complete, a fraction of a k-block's conversion time).
   static constexpr int PS = NT == 2 ? 3 : 2;
-  static constexpr int FIXED = 1024 + Tr::STAGING_BYTES + 512;
+  static constexpr int STAGING_PER_WARP = 32 * 32 * 4;  // one FP32 epilogue block per warp
+  static constexpr int STAGING_BYTES = ACC_WARPS * STAGING_PER_WARP;
+  static constexpr int FIXED = 1024 + STAGING_BYTES + 512;
   static constexpr int RS_FIT = (kSmemBudget - FIXED - PS * PLANE_BYTES) / RAW_BYTES;
   static constexpr int RS = RS_FIT > 6 ? 6 : RS_FIT;  // raw stages
   static_assert(RS >= 2 + G, "raw ring: loads in flight beside the tiles in conversion");
@@ -142,7 +144,7 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
   uint8_t* planes = smem;
   uint8_t* raws = planes + PS * F::PLANE_BYTES;
   uint8_t* staging = raws + RS * F::RAW_BYTES;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + Tr::STAGING_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + F::STAGING_BYTES);
   uint64_t* full = bars;                // plane stage converted (rank 0: both CTAs' converters)
   uint64_t* empty = full + PS;          // plane stage read by the MMAs (commit, both CTAs)
   uint64_t* raw_full = empty + PS;      // raw tile landed (TMA bytes)
@@ -255,7 +257,7 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
     constexpr int W = Tr::COLS_PER_EW;
     const int colsub = ((warp - 2) / 4) * W;
     const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
-    uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
+    uint8_t* stg = staging + (warp - 2) * F::STAGING_PER_WARP;
     const uint32_t tempty_rank0 = mapa_shared(smem_u32(&tempty[0]), 0);
     int ci = 0;
     for (int unit = unit0; unit < units; unit += unit_step) {
@@ -370,7 +372,9 @@ struct FusedInplaceCfg {
   static constexpr int ACC_WARPS = 8, CONV_WARPS = 6, CONV_WARP0 = 2 + ACC_WARPS;
   static constexpr int THREADS = (CONV_WARP0 + CONV_WARPS) * 32;
   static constexpr int MAX_REGS = 16384 / (32 * ((THREADS / 32 + 3) / 4)) / 8 * 8;
-  static constexpr int FIXED = 1024 + Tr::STAGING_BYTES + 512;
+  static constexpr int STAGING_PER_WARP = 32 * 32 * 4;  // one FP32 epilogue block per warp
+  static constexpr int STAGING_BYTES = ACC_WARPS * STAGING_PER_WARP;
+  static constexpr int FIXED = 1024 + STAGING_BYTES + 512;
   static constexpr int NS_FIT = (kSmemBudget - FIXED) / STAGE;
   static constexpr int NS = NS_FIT > 6 ? 6 : NS_FIT;
   static_assert(NS >= 3, "stage ring");
@@ -448,7 +452,7 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* stages = smem;
   uint8_t* staging = stages + NS * F::STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + Tr::STAGING_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(staging + F::STAGING_BYTES);
   uint64_t* raw_full = bars;       // FP32 tiles landed (TMA bytes)
   uint64_t* full = raw_full + NS;  // planes written (rank 0: both CTAs' converters)
   uint64_t* empty = full + NS;     // planes read by the MMAs (commit, both CTAs)
@@ -577,7 +581,7 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
     constexpr int W = Tr::COLS_PER_EW;
     const int colsub = ((warp - 2) / 4) * W;
     const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
-    uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
+    uint8_t* stg = staging + (warp - 2) * F::STAGING_PER_WARP;
     const uint32_t tempty_rank0 = mapa_shared(smem_u32(&tempty[0]), 0);
     int ci = 0;
     for (int unit = unit0; unit < units; unit += unit_step) {

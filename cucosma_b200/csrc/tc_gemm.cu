@@ -104,17 +104,17 @@ static Tiling make_tiling(const Plan& pl, int slices, int bn, const cucosma_gemm
 // The fused split pays off when the separate pre-pass (read the FP32
 // operands, write nt BF16 planes) would take more than a quarter of the
 // GEMM's own bound (tensor time at nt products of BF16, or the HBM time of
-// reading the planes and writing -- with beta, also reading -- C), and the
-// C traffic is small beside the operands' (the converter warps also run the
-// epilogue, so a C-heavy shape such as 256 x 1,048,576 x 256 would serialise
-// its stores with the next tile's conversion): operands read only a few
-// times with a small output, as in the large-K family.
+// reading the planes and writing -- with beta, also reading -- C): operands
+// read only a few times, as in the large-K and large-N families (measured on
+// B200, BF16x3, beta 0.5: 256 x 256 x 1,048,576 0.55 ms fused against about
+// 1.2 ms; 256 x 1,048,576 x 256 0.98 against 1.23 ms), and not where small
+// operands are re-read by many tiles (16384 x 16384 x 256: 0.89 fused against
+// 0.72 ms with the pre-pass, whose cost there is negligible).
 static bool fused_pays(const cucosma_gemm_desc* d, int nt) {
   const double M = (double)d->m, N = (double)d->n, K = (double)d->k;
   const double hbm = 6.5e12, bf16 = 1.6e15;
   const double products = nt == 2 ? 3.0 : 6.0;
-  const double c_bytes = M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0), ab_bytes = (M * K + K * N) * 4.0;
-  if (c_bytes > 0.25 * ab_bytes) return false;
+  const double c_bytes = M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0);
   const double t_pre = (M * K + K * N) * (4.0 + 2.0 * nt) / hbm;
   const double t_mma = 2.0 * M * N * K * products / bf16;
   const double t_mem = ((M * K + K * N) * 2.0 * nt + c_bytes) / hbm;

@@ -84,7 +84,8 @@ struct OutCtx {
   const int32_t* ea;
   const int32_t* eb;
   const CUtensorMap* tmc;  // non-null: the FP32 epilogue moves C by TMA
-  uint64_t* tbar;          // this epilogue warp's barrier for its C loads
+  uint64_t* tbar;          // this epilogue warp's barriers for its C loads (one per staging block)
+  int stg_blocks;          // 32 x 32 staging blocks this warp has (1 or 2)
   WaitCtl ctl;
 };
 

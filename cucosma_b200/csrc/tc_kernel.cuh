@@ -137,6 +137,7 @@ __device__ __forceinline__ OutCtx out_ctx(const TcParams& p, const Unit& u) {
   o.beta = p.beta;
   o.ctl = p.ctl;
   o.tbar = nullptr;
+  o.stg_blocks = 1;
   o.tmc = (u.group < 0 && p.tma_out && !p.partial) ? &p.tmc : nullptr;
   if (u.group < 0) {
     o.m = p.m;
@@ -261,10 +262,10 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
   uint64_t* tfull = bars + 2 * ST;
   uint64_t* tempty = tfull + 4;
   uint64_t* drain = tempty + 4;
-  uint64_t* ebar = drain + 1;  // one per epilogue warp: its TMA loads of C
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + Tr::EPI_WARPS);
+  uint64_t* ebar = drain + 1;  // two per epilogue warp: its TMA loads of C (one per staging block)
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + 2 * Tr::EPI_WARPS);
   static_assert(NBUF <= 4, "accumulator buffers");
-  static_assert((2 * ST + 9 + Tr::EPI_WARPS) * 8 + 4 <= 512, "barrier area");
+  static_assert((2 * ST + 9 + 2 * Tr::EPI_WARPS) * 8 + 4 <= 512, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.ngroups > 0 ? p.total_tiles : p.tiles_m * p.tiles_n * p.splits;
@@ -288,7 +289,7 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
       mbar_init(&tempty[b], Tr::EPI_WARPS * (PAIR ? 2 : 1));  // rank 0's: released by both CTAs' epilogues
     }
     mbar_init(drain, 1);
-    for (int w = 0; w < Tr::EPI_WARPS; ++w) mbar_init(&ebar[w], 1);
+    for (int w = 0; w < 2 * Tr::EPI_WARPS; ++w) mbar_init(&ebar[w], 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -468,7 +469,8 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
       // the output context is built where it is used (fewer registers held across the chunk loop)
       auto octx = [&]() {
         OutCtx o = out_ctx(p, u);
-        o.tbar = &ebar[warp - 2];
+        o.tbar = &ebar[2 * (warp - 2)];
+        o.stg_blocks = Tr::STAGING_PER_WARP / (32 * 32 * 4);
         return o;
       };
       if constexpr (Tr::PROMOTE) {
@@ -531,7 +533,7 @@ struct EpiF32 {
   // (the 128-byte swizzle TMA uses; the buffer is 1024-byte aligned).  Rows
   // are read and written as float4 chunks by the lane owning the row, and
   // columns one float per lane -- both free of bank conflicts.
-  static constexpr int STAGING_PER_WARP = 32 * 32 * 4;
+  static constexpr int STAGING_PER_WARP = 2 * 32 * 32 * 4;  // two blocks: C loads overlap the previous block
   static __device__ __forceinline__ int sw(int r, int c) { return r * 32 + ((((c >> 2) ^ (r & 7))) << 2) + (c & 3); }
 
   // This lane's row of the block: epi(alpha * acc + beta * C) with C read
@@ -698,11 +700,62 @@ struct EpiF32 {
     }
   }
 
+  // TMA path with two staging blocks: block i + 1's C load is in flight
+  // while block i is combined and stored (each buffer is reloaded once the
+  // store issued from it two blocks earlier has read it).
+  template <int BN>
+  static __device__ __forceinline__ void finish_tma2(const OutCtx& p, const float (&master)[BN], float* stg, int lane,
+                                                     int row0, int col0) {
+    const float alpha = (float)p.alpha, beta = (float)p.beta;
+    const bool ld = beta != 0.f;
+    if (lane == 0) bulk_wait_read_all();  // the previous tile's stores have read both blocks
+    __syncwarp();
+    uint64_t tok[2] = {0, 0};
+    if (ld && lane == 0 && col0 < p.n) {
+      tok[0] = mbar_arrive_expect_tx_token(&p.tbar[0], 32 * 32 * 4);
+      tma_load_2d(stg, p.tmc, col0, row0, &p.tbar[0]);
+    }
+#pragma unroll
+    for (int i = 0; i < BN / 32; ++i) {
+      const int col = col0 + 32 * i;
+      if (col >= p.n) break;
+      float* b = stg + (i & 1) * (32 * 32);
+      if (ld) {
+        if (lane == 0 && !mbar_wait_token(&p.tbar[i & 1], tok[i & 1], kErrTimeoutOutput, p.ctl))
+          mbar_wait_token(&p.tbar[i & 1], tok[i & 1], kErrTimeoutDrain, p.ctl);
+        __syncwarp();
+      } else if (i >= 2) {
+        if (lane == 0) bulk_wait_read_but_last();  // the store from this block two steps ago has read it
+        __syncwarp();
+      }
+      float acc[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = master[32 * i + j];
+      combine_row(p.epilogue, reinterpret_cast<float4*>(b) + lane * 8, acc, alpha, beta, lane);
+      fence_proxy_async_smem();  // the block is read by TMA (async proxy)
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_2d(p.tmc, b, col, row0);
+        bulk_commit();
+        if (ld && i + 1 < BN / 32 && col + 32 < p.n) {
+          bulk_wait_read_but_last();  // the other block's previous store has read it
+          float* nb = stg + ((i + 1) & 1) * (32 * 32);
+          tok[(i + 1) & 1] = mbar_arrive_expect_tx_token(&p.tbar[(i + 1) & 1], 32 * 32 * 4);
+          tma_load_2d(nb, p.tmc, col + 32, row0, &p.tbar[(i + 1) & 1]);
+        }
+      }
+    }
+  }
+
   template <int BN>
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[BN], uint8_t* stg_raw,
                                                 int lane, int row0, int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
     if (p.tmc != nullptr) {
+      if (p.stg_blocks >= 2) {
+        finish_tma2<BN>(p, master, stg, lane, row0, col0);
+        return;
+      }
 #pragma unroll
       for (int c0 = 0; c0 < BN; c0 += 32) {
         float acc[32];
