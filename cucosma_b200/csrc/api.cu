@@ -361,7 +361,7 @@ cucosma_status gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B,
     return fp32 ? run_native<float>(d, pl, (const float*)A, (const float*)B, (float*)C, ws, di, st)
                 : run_native<double>(d, pl, (const double*)A, (const double*)B, (double*)C, ws, di, st);
   }
-  return tc_gemm_ex(d, A, B, C, ws, di, st, prep);
+  return tc_gemm_ex(d, A, B, C, ws, ws_bytes, di, st, prep);
 }
 
 // ---------------------------------------------- launch count and profiling

@@ -54,15 +54,15 @@ cucosma_status tc_workspace_size(const cucosma_gemm_desc* d, size_t* bytes, cons
 void tc_plan_info(const cucosma_gemm_desc* d, const DeviceInfo* di, cucosma_plan_info* info, bool allow_fused = true);
 // Whether a plain call with *d runs the fused-split kernel.
 bool tc_plan_is_fused(const cucosma_gemm_desc* d, const DeviceInfo* di);
-cucosma_status tc_gemm(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
-                       const DeviceInfo* di, cudaStream_t st);
 // prep: which operand pre-passes run (kPrepA | kPrepB for a plain call).  An
 // operand left out must already be in ws at the plan's offsets -- written by
 // the caller (the backward pass), or by an earlier call on the same B (row
 // blocks of one problem: B's planes / slices, exponents and magnitude sums
 // sit first in the workspace and depend on N, K and the slice layout only).
+// ws_bytes: the caller's workspace size; the plan actually run must fit it
+// (WORKSPACE_TOO_SMALL otherwise, before anything is launched).
 cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void* B, void* C, void* ws,
-                          const DeviceInfo* di, cudaStream_t st, int prep);
+                          size_t ws_bytes, const DeviceInfo* di, cudaStream_t st, int prep);
 
 // The native tile kernel (no skinny-shape kernels) with plan pl; with a gate
 // every kernel it enqueues runs only if *gate == gate_value on the device.

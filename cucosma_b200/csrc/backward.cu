@@ -132,7 +132,7 @@ extern "C" cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* f, cons
                           di->sms, st) != cudaSuccess)
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     note_launches(2);
-    if ((s = tc_gemm_ex(d, nullptr, nullptr, dA, workspace, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
+    if ((s = tc_gemm_ex(d, nullptr, nullptr, dA, workspace, workspace_bytes, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
   }
   if (dB) {
     // dB (k x n) = A^T (k x m) * G (m x n): K' = m.
@@ -146,7 +146,7 @@ extern "C" cucosma_status cucosma_gemm_backward(const cucosma_gemm_desc* f, cons
                           scale) != cudaSuccess)
       return CUCOSMA_STATUS_LAUNCH_FAILED;
     note_launches(2);
-    if ((s = tc_gemm_ex(d, nullptr, nullptr, dB, workspace, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
+    if ((s = tc_gemm_ex(d, nullptr, nullptr, dB, workspace, workspace_bytes, di, st, 0)) != CUCOSMA_STATUS_SUCCESS) return s;
   }
   return CUCOSMA_STATUS_SUCCESS;
 }

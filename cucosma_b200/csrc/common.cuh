@@ -40,9 +40,24 @@ enum Epilogue : int { kEpiNone = 0, kEpiSigmoid = 1, kEpiRelu = 2 };
 // holds the reference's ReLU / Sigmoid loops; sigmoid4.cuh:19-22 the formula).
 // epi_t<EPI>: the activation fixed at compile time, for epilogues that
 // dispatch once per block.
+// FP32 sigmoid 1 / (1 + e^-v) without a division: the reciprocal of
+// x = 1 + e^-v (x >= 1) from the hardware approximation refined by one
+// Newton-Raphson step r <- r + r (1 - x r), which squares its relative error
+// (from about 2^-23 to below 2^-44, so the result is within an ulp of the
+// correctly rounded quotient); x = +inf (v below about -88) gives 0.  The
+// IEEE division it replaces carries an out-of-line slow path whose call
+// sites made the tensor-core epilogue (128 live accumulator registers a
+// thread) several times slower on B200.
+__device__ __forceinline__ float sigmoid_f32(float v) {
+  const float x = 1.0f + expf(-v);
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  r = fmaf(r, fmaf(-x, r, 1.0f), r);
+  return x == __int_as_float(0x7f800000) ? 0.0f : r;
+}
 template <int EPI>
 __device__ __forceinline__ float epi_t(float v) {
-  if constexpr (EPI == kEpiSigmoid) return 1.0f / (1.0f + expf(-v));
+  if constexpr (EPI == kEpiSigmoid) return sigmoid_f32(v);
   else if constexpr (EPI == kEpiRelu) return fmaxf(v, 0.0f);
   else return v;
 }
@@ -56,11 +71,11 @@ __device__ __forceinline__ double epi_t(double v) {
 // inlined: inlined, the compiler if-converted it, evaluating the exponential
 // and the division for every element of every epilogue (that made the FP32
 // tensor-core epilogue five times slower on B200 with no activation at all).
-__device__ __noinline__ float sigmoid_f32(float v);
+__device__ __noinline__ float sigmoid_f32_call(float v);
 __device__ __noinline__ double sigmoid_f64(double v);
 __device__ __forceinline__ float apply_epi(float v, int epi) {
   if (epi == kEpiRelu) return fmaxf(v, 0.0f);
-  if (epi == kEpiSigmoid) return sigmoid_f32(v);
+  if (epi == kEpiSigmoid) return sigmoid_f32_call(v);
   return v;
 }
 __device__ __forceinline__ double apply_epi(double v, int epi) {
@@ -68,7 +83,7 @@ __device__ __forceinline__ double apply_epi(double v, int epi) {
   if (epi == kEpiSigmoid) return sigmoid_f64(v);
   return v;
 }
-__device__ __noinline__ inline float sigmoid_f32(float v) { return epi_t<kEpiSigmoid>(v); }
+__device__ __noinline__ inline float sigmoid_f32_call(float v) { return sigmoid_f32(v); }
 __device__ __noinline__ inline double sigmoid_f64(double v) { return epi_t<kEpiSigmoid>(v); }
 
 // alpha/beta combination.  The reference scales the accumulator by ALPHA

@@ -418,8 +418,8 @@ def test_fused_split_forced_split_k(precision, ftile, utile):
 
 def test_fused_split_chosen_for_large_k():
     """Auto planning picks the fused kernel where the operands are read about
-    once (256 x 256 x 262144, 256 x 262144 x 256) and not for a square
-    problem or a flat one whose small operands many tiles re-read."""
+    once (256 x 256 x 262144; for BF16x3 also 256 x 262144 x 256) and not for
+    a square problem or a flat one whose small operands many tiles re-read."""
     import torch
 
     for prec in ("bf16x3", "bf16x6"):
@@ -427,11 +427,34 @@ def test_fused_split_chosen_for_large_k():
         B = torch.empty((262144, 256), device="cuda")
         Cm = torch.empty((256, 256), device="cuda")
         assert cc.get_plan(cc.make_desc(A, B, Cm, precision=prec))["fused"] == 1
-        Cn = torch.empty((256, 262144), device="cuda")
-        assert cc.get_plan(cc.make_desc(Cm, A, Cn, 1.0, 0.5, precision=prec))["fused"] == 1
+        Cn = torch.empty((256, 262144), device="cuda")  # C-heavy: only BF16x3's in-place kernel pays there
+        assert cc.get_plan(cc.make_desc(Cm, A, Cn, 1.0, 0.5, precision=prec))["fused"] == (prec == "bf16x3")
         S = torch.empty((4096, 4096), device="cuda")
         assert cc.get_plan(cc.make_desc(S, S, S, precision=prec))["fused"] == 0
         F = torch.empty((16384, 256), device="cuda")
         Ft = torch.empty((256, 16384), device="cuda")
         Cf = torch.empty((16384, 16384), device="cuda")
         assert cc.get_plan(cc.make_desc(F, Ft, Cf, 1.0, 0.5, precision=prec))["fused"] == 0
+
+
+@pytest.mark.parametrize("precision", ["native", "bf16x6", "bf16x3"])
+def test_sigmoid_epilogue_accuracy(precision):
+    """The fused sigmoid (exponential, then a Newton-refined hardware
+    reciprocal instead of an IEEE division) against the FP64 sigmoid over
+    [-100, 100] and special values: with K = 1 and B = 1 the product is the
+    FP32 value itself (exact for BF16x6; BF16x3 is checked on values exact in
+    BF16), so the error is the epilogue's alone.
+    Within 4 ulp of the FP64 value, or 1e-37 absolute where it underflows."""
+    v = np.concatenate([np.linspace(-100, 100, 8000), [0.0, -0.0, 1e-30, -1e-30, 88.0, -87.0, -88.5, -89.0, -104.0,
+                                                       16.6, -16.6, 1e-4, -1e-4]]).astype(np.float32)
+    if precision == "bf16x3":
+        v = (v.astype(np.float32).view(np.uint32) & np.uint32(0xFFFF0000)).view(np.float32)
+    m = len(v)
+    A = v.reshape(m, 1)
+    B = np.ones((1, 4), np.float32)
+    Cin = np.zeros((m, 4), np.float32)
+    out = run(A, B, Cin, 1.0, 0.0, precision, epilogue="sigmoid")[0]
+    ref = 1.0 / (1.0 + np.exp(-v.astype(np.float64)))
+    err = np.abs(out.astype(np.float64) - ref[:, None])
+    ulp = np.spacing(ref.astype(np.float32)).astype(np.float64)[:, None]
+    assert np.all((err <= 4 * ulp) | (err <= 1e-37)), float((err / ulp).max())
