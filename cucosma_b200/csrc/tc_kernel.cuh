@@ -263,9 +263,10 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
   uint64_t* tempty = tfull + 4;
   uint64_t* drain = tempty + 4;
   uint64_t* ebar = drain + 1;  // two per epilogue warp: its TMA loads of C (one per staging block)
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + 2 * Tr::EPI_WARPS);
+  uint64_t* tfwd = ebar + 2 * Tr::EPI_WARPS;  // pair, rank 1: its epilogue released accumulator b (forwarded)
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(tfwd + 4);
   static_assert(NBUF <= 4, "accumulator buffers");
-  static_assert((2 * ST + 9 + 2 * Tr::EPI_WARPS) * 8 + 4 <= 512, "barrier area");
+  static_assert((2 * ST + 13 + 2 * Tr::EPI_WARPS) * 8 + 4 <= 512, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.ngroups > 0 ? p.total_tiles : p.tiles_m * p.tiles_n * p.splits;
@@ -286,7 +287,9 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
     }
     for (int b = 0; b < 4; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], Tr::EPI_WARPS * (PAIR ? 2 : 1));  // rank 0's: released by both CTAs' epilogues
+      // rank 0's: released by its epilogue warps and, in a pair, by rank 1's forwarder
+      mbar_init(&tempty[b], Tr::EPI_WARPS + (PAIR ? 1 : 0));
+      mbar_init(&tfwd[b], Tr::EPI_WARPS);
     }
     mbar_init(drain, 1);
     for (int w = 0; w < 2 * Tr::EPI_WARPS; ++w) mbar_init(&ebar[w], 1);
@@ -426,6 +429,34 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
         commit_self<PAIR>(drain);  // wait (bounded) for every MMA issued so far
         mbar_wait(drain, 0, kErrTimeoutDrain, p.ctl);
       }
+    } else if (PAIR && lane == 0) {
+      // Rank 1: forward each accumulator release of this CTA's epilogue
+      // warps to rank 0 with one cluster-scope arrival (a release at cluster
+      // scope costs a warp about 1700 cycles on B200; paid here, once, off
+      // the epilogue warps' path).  Same release sequence as the epilogue.
+      const uint32_t tempty0 = mapa_shared(smem_u32(&tempty[0]), 0);
+      auto forward = [&](int idx, uint32_t parity) {
+        if (!mbar_wait(&tfwd[idx], parity, kErrTimeoutAccum, p.ctl)) return false;
+        mbar_arrive_cluster(tempty0 + (uint32_t)(idx * sizeof(uint64_t)));
+        return true;
+      };
+      int ci = 0;
+      bool ok = true;
+      for (int unit = unit0; unit < units && ok; unit += unit_step) {
+        Unit u;
+        resolve_unit(p, &tmA, &tmB, unit, u);
+        if constexpr (Tr::PROMOTE) {
+          for (int cs = u.kb0; cs < u.kb1 && ok; cs += chunk, ++ci) {
+            if constexpr (Tr::SPLIT)
+              ok = forward(1, ci & 1) && forward(0, ci & 1);
+            else
+              ok = forward(ci % NBUF, (ci / NBUF) & 1);
+          }
+        } else {
+          ok = forward(ci % NBUF, (ci / NBUF) & 1);
+          ++ci;
+        }
+      }
     }
   } else {
     // ---------------------------------------------------------- epilogue
@@ -437,16 +468,12 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
     const int colsub = ((warp - 2) / 4) * W;
     const uint32_t lane_base = tmem_base + ((uint32_t)(32 * q) << 16);
     uint8_t* stg = staging + (warp - 2) * Tr::STAGING_PER_WARP;
-    // Releasing an accumulator: arrive on rank 0's tempty barrier idx.
+    // Releasing an accumulator: arrive on tempty[idx] (rank 0), or on the
+    // local tfwd[idx] that rank 1's forwarder hands on to rank 0.
     auto release = [&](int idx) {
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) {
-        if constexpr (PAIR)
-          mbar_arrive_cluster(mapa_shared(smem_u32(&tempty[idx]), 0));
-        else
-          mbar_arrive(&tempty[idx]);
-      }
+      if (lane == 0) mbar_arrive(rank == 0 ? &tempty[idx] : &tfwd[idx]);
     };
     int ci = 0;
     bool ok = true;
