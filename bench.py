@@ -66,7 +66,7 @@ def dram_traffic(path, n):
         with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
             for line in f:
                 t = line.split()
-                if len(t) >= 5 and not t[0].startswith("#") and t[0] == path and int(t[1]) == n:
+                if len(t) >= 5 and not t[0].startswith("#") and t[0] == path and t[1] == str(n):
                     return int(t[3]) + int(t[4])
     except (OSError, ValueError):
         pass
@@ -707,6 +707,44 @@ def reference_gpu_kernel(n, steps, warmup):
 
 
 # -------------------------------------------------------------------- main
+def shape_run(args):
+    """One GEMM shape through the library's default plan (--shape M,N,K), for
+    profiling: W warm-up and K timed calls on uniform[-1, 1] inputs, CUDA
+    events on the current stream; prints the plan and the time per call."""
+    import torch
+
+    import cucosma_b200 as cc
+
+    m, n, k = (int(x) for x in args.shape.split(","))
+    dt = torch.float64 if args.precision == "ozaki" or args.precision == "native_f64" else torch.float32
+    prec = "native" if args.precision.startswith("native") else args.precision
+    A = make_rect(m, k, 100, dt)
+    B = make_rect(k, n, 101, dt)
+    C = make_rect(m, n, 102, dt)
+    d = cc.make_desc(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue)
+    ws = cc.alloc_workspace(d)
+
+    def call():
+        cc.gemm(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue, workspace=ws)
+
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    es = 4 if dt == torch.float32 else 8
+    gb = es * (m * k + k * n + (2 if args.beta else 1) * m * n) / 1e9
+    print(json.dumps({"shape": [m, n, k], "precision": args.precision, "beta": args.beta, "epilogue": args.epilogue,
+                      "ms": ms, "tflops": 2.0 * m * n * k / ms / 1e9, "algorithmic_tb_s": gb / ms,
+                      "plan": cc.get_plan(d)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -722,12 +760,19 @@ def main():
     ap.add_argument("--sweep-sizes", default="8192,16384")
     ap.add_argument("--no-families", action="store_true", help="skip the reference shape families")
     ap.add_argument("--family-steps", type=int, default=3)
+    ap.add_argument("--shape", default="", help="M,N,K: time one GEMM of this shape (profiling runs; with "
+                    "--precision, --beta, --epilogue) and print its plan and time instead of the bench line")
+    ap.add_argument("--precision", default="bf16x3")
+    ap.add_argument("--beta", type=float, default=0.5)
+    ap.add_argument("--epilogue", default="none")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return reference_arm(args)
     if args.precision_sweep:
         return precision_sweep(args)
+    if args.shape:
+        return shape_run(args)
 
     import torch
 
