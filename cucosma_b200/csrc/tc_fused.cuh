@@ -294,7 +294,7 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
       prefetch_unit(unit + unit_step);
       OutCtx o = out_ctx(p, u);
       o.tbar = &ebar[warp - 2];
-      Tr::finish(o, master, stg, lane, row0, col0 + colsub, u.z);
+      Tr::template finish<1>(o, master, stg, lane, row0, col0 + colsub, u.z);
       ci += nchunks;
     }
     if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed
@@ -618,7 +618,7 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
       prefetch_unit(unit + unit_step);
       OutCtx o = out_ctx(p, u);
       o.tbar = &ebar[warp - 2];
-      Tr::finish(o, master, stg, lane, row0, col0 + colsub, u.z);
+      Tr::template finish<1>(o, master, stg, lane, row0, col0 + colsub, u.z);
       ci += nchunks;
     }
     if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed

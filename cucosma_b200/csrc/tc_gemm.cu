@@ -301,9 +301,20 @@ TcParams tc_params(const cucosma_gemm_desc* d, const Tiling& t, const Plan& pl, 
     if (tma_epilogue && pl.kind != 2 && C != nullptr && (reinterpret_cast<uintptr_t>(C) & 15) == 0 &&
         (d->ldc * 4) % 16 == 0 && d->n % 4 == 0)
       p.tma_out = encode_2d(&p.tmc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)d->n, (uint64_t)d->m,
-                            (uint64_t)d->ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B)
+                            (uint64_t)d->ldc, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B) &&
+                          encode_2d(&p.tmc_pf, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, (uint64_t)d->n,
+                                    (uint64_t)d->m, (uint64_t)d->ldc, 64, 32, CU_TENSOR_MAP_SWIZZLE_NONE)
                       ? 1
                       : 0;
+    static const bool tma_wide = [] {
+      const char* e = std::getenv("CUCOSMA_TMA_WIDE");
+      return !(e && e[0] == '0');
+    }();
+    if (p.tma_out && tma_wide && d->n % 32 == 0)
+      p.tma_wide = encode_3d(&p.tmc3, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, 32, (uint64_t)d->n / 32, (uint64_t)d->m,
+                             32, (uint64_t)d->ldc, 32, 2, 32, CU_TENSOR_MAP_SWIZZLE_128B)
+                       ? 1
+                       : 0;
   }
   return p;
 }

@@ -46,7 +46,14 @@ struct TcParams {
   // swizzle; used by the epilogue for whole-problem outputs (not split-K
   // partials, not grouped launches).
   CUtensorMap tmc;
-  int tma_out;
+  // The same C with 64-column boxes (no swizzle), for L2 prefetches only:
+  // 256-byte row requests (128-byte ones cap a stream near 4.6 TB/s on B200).
+  CUtensorMap tmc_pf;
+  // With N a multiple of 32: C as {32 columns, N / 32 column chunks, M rows}
+  // with [32 rows][2 chunks][32] boxes (128-byte swizzle per 128-byte line),
+  // so the epilogue's loads and stores are 256-byte row requests.
+  CUtensorMap tmc3;
+  int tma_out, tma_wide;
   int m, n, k;
   int tiles_m, tiles_n;
   int kblocks;       // k-blocks of the whole K
@@ -83,7 +90,9 @@ struct OutCtx {
   int64_t ldo, ws_split_stride;
   const int32_t* ea;
   const int32_t* eb;
-  const CUtensorMap* tmc;  // non-null: the FP32 epilogue moves C by TMA
+  const CUtensorMap* tmc;     // non-null: the FP32 epilogue moves C by TMA
+  const CUtensorMap* tmc_pf;  // its 64-column prefetch boxes
+  const CUtensorMap* tmc3;    // non-null: 64-column 3-D boxes (needs two staging blocks)
   uint64_t* tbar;          // this epilogue warp's barriers for its C loads (one per staging block)
   int stg_blocks;          // 32 x 32 staging blocks this warp has (1 or 2)
   WaitCtl ctl;

@@ -114,7 +114,7 @@ __device__ __forceinline__ void prefetch_c_block(const OutCtx& o, int row0, int 
     // epilogue's own proxy fences then have no prefetches of their own to
     // wait for)
     if (lane == 0)
-      for (int c = col0; c < col0 + cols && c < o.n; c += 32) tma_prefetch_2d(o.tmc, c, row0);
+      for (int c = col0; c < col0 + cols && c < o.n; c += 64) tma_prefetch_2d(o.tmc_pf, c, row0);
     return;
   }
   const int c1 = min(o.n, col0 + cols);
@@ -139,6 +139,8 @@ __device__ __forceinline__ OutCtx out_ctx(const TcParams& p, const Unit& u) {
   o.tbar = nullptr;
   o.stg_blocks = 1;
   o.tmc = (u.group < 0 && p.tma_out && !p.partial) ? &p.tmc : nullptr;
+  o.tmc_pf = &p.tmc_pf;
+  o.tmc3 = (o.tmc != nullptr && p.tma_wide) ? &p.tmc3 : nullptr;
   if (u.group < 0) {
     o.m = p.m;
     o.n = p.n;
@@ -561,6 +563,12 @@ struct EpiF32 {
   // are read and written as float4 chunks by the lane owning the row, and
   // columns one float per lane -- both free of bank conflicts.
   static constexpr int STAGING_PER_WARP = 2 * 32 * 32 * 4;  // two blocks: C loads overlap the previous block
+  // Columns c0 .. c0 + 31 of a register accumulator row, as a 32-array (c0
+  // is a compile-time constant at every use, so no copy is made).
+  template <int BN>
+  static __device__ __forceinline__ const float (&cols32(const float (&m)[BN], int c0))[32] {
+    return *reinterpret_cast<const float(*)[32]>(&m[c0]);
+  }
   static __device__ __forceinline__ int sw(int r, int c) { return r * 32 + ((((c >> 2) ^ (r & 7))) << 2) + (c & 3); }
 
   // This lane's row of the block: epi(alpha * acc + beta * C) with C read
@@ -755,10 +763,7 @@ struct EpiF32 {
         if (lane == 0) bulk_wait_read_but_last();  // the store from this block two steps ago has read it
         __syncwarp();
       }
-      float acc[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) acc[j] = master[32 * i + j];
-      combine_row(p.epilogue, reinterpret_cast<float4*>(b) + lane * 8, acc, alpha, beta, lane);
+      combine_row(p.epilogue, reinterpret_cast<float4*>(b) + lane * 8, cols32(master, 32 * i), alpha, beta, lane);
       fence_proxy_async_smem();  // the block is read by TMA (async proxy)
       __syncwarp();
       if (lane == 0) {
@@ -774,13 +779,55 @@ struct EpiF32 {
     }
   }
 
+  // 64-column blocks through the 3-D map: one 8 KB staging block [32 rows]
+  // [2 chunks][32] (line 2r + h of row r, chunk h, 128-byte swizzle), one box
+  // load of C (beta != 0) and one box store per block, 256-byte rows each.
   template <int BN>
+  static __device__ __forceinline__ void finish_tma_wide(const OutCtx& p, const float (&master)[BN], float* stg,
+                                                         int lane, int row0, int col0) {
+    const float alpha = (float)p.alpha, beta = (float)p.beta;
+    float4* s4 = reinterpret_cast<float4*>(stg);
+#pragma unroll
+    for (int i = 0; i < BN / 64; ++i) {
+      const int col = col0 + 64 * i;
+      if (col >= p.n) break;
+      if (lane == 0) bulk_wait_read_all();  // the previous block's store has read the buffer
+      __syncwarp();
+      if (beta != 0.f) {
+        if (lane == 0) {
+          const uint64_t token = mbar_arrive_expect_tx_token(&p.tbar[0], 2 * 32 * 32 * 4);
+          tma_load_3d(stg, p.tmc3, 0, col / 32, row0, &p.tbar[0]);
+          if (!mbar_wait_token(&p.tbar[0], token, kErrTimeoutOutput, p.ctl))
+            mbar_wait_token(&p.tbar[0], token, kErrTimeoutDrain, p.ctl);
+        }
+        __syncwarp();
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int line = 2 * lane + h;
+        combine_row(p.epilogue, s4 + line * 8, cols32(master, 64 * i + 32 * h), alpha, beta, line);
+      }
+      fence_proxy_async_smem();  // the block is read by TMA (async proxy)
+      __syncwarp();
+      if (lane == 0) {
+        tma_store_3d(p.tmc3, stg, 0, col / 32, row0);
+        bulk_commit();
+      }
+    }
+  }
+
+  // STG: 32 x 32 staging blocks the warp has (2 in tc_gemm_kernel, 1 in the
+  // fused kernels), fixed at compile time so only the matching paths exist.
+  template <int BN, int STG>
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[BN], uint8_t* stg_raw,
                                                 int lane, int row0, int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
     if (p.tmc != nullptr) {
-      if (p.stg_blocks >= 2) {
-        finish_tma2<BN>(p, master, stg, lane, row0, col0);
+      if constexpr (STG >= 2) {
+        if (p.tmc3 != nullptr && BN % 64 == 0)
+          finish_tma_wide<BN>(p, master, stg, lane, row0, col0);
+        else
+          finish_tma2<BN>(p, master, stg, lane, row0, col0);
         return;
       }
 #pragma unroll
@@ -957,9 +1004,10 @@ struct TraitsBase {
   static __device__ __forceinline__ void accumulate_one(uint32_t tacc, int d, float (&master)[COLS_PER_EW]) {
     if constexpr (PROMOTE) Epi::template accumulate<COLS_PER_EW, BN, 1>(tacc + (uint32_t)(d * BN), master);
   }
+  template <int STG = STAGING_PER_WARP / 4096>
   static __device__ __forceinline__ void finish(const OutCtx& p, const float (&master)[COLS_PER_EW], uint8_t* stg,
                                                 int lane, int row0, int col0, int z) {
-    if constexpr (PROMOTE) Epi::template finish<COLS_PER_EW>(p, master, stg, lane, row0, col0, z);
+    if constexpr (PROMOTE) Epi::template finish<COLS_PER_EW, STG>(p, master, stg, lane, row0, col0, z);
   }
 };
 

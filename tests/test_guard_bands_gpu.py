@@ -27,6 +27,8 @@ CASES = [  # (precision, dtype, m, n, k, split_k[, tile])
     # N a multiple of 4: C leaves through TMA boxes (partial tiles right and below)
     ("bf16x3", np.float32, 129, 260, 65, 0), ("bf16x6", np.float32, 130, 72, 45, 0),
     ("bf16x3", np.float32, 300, 132, 3000, 0, 5), ("bf16x6", np.float32, 300, 132, 3000, 0, 4),
+    # N a multiple of 32 with an odd number of 32-column chunks: 64-column 3-D boxes, the last half outside
+    ("bf16x3", np.float32, 129, 96, 65, 0), ("bf16x6", np.float32, 260, 160, 45, 0),
 ]
 
 
