@@ -359,7 +359,10 @@ __global__ void __maxnreg__((FusedCfg<Tr, G>::MAX_REGS))
 // so four stages give two in flight, one in conversion and one in the MMAs.
 // Roles as in tc_fused_kernel (producer, MMA issuer, 8 promotion/epilogue
 // warps, 6 converter warps: 4 for A, 2 for B).
-template <class Tr>
+// STG: 32 x 32 FP32 staging blocks per epilogue warp.  1: four stages (the
+// large-K shapes, whose small C leaves once); 2: three stages and the
+// unfused kernels' 64-column C boxes (the C-heavy large-N shapes).
+template <class Tr, int STG = 1>
 struct FusedInplaceCfg {
   static_assert(Tr::PAIR && !Tr::PACKED && !Tr::SPLIT && Tr::NBUF >= 2 && Tr::SWZ == 64 && Tr::EPI_WARPS == 8 &&
                     Tr::BN_LOCAL == 64 && Tr::COLS_PER_EW == 64 && Tr::NA == 2 && Tr::CHUNK % 2 == 0,
@@ -372,7 +375,7 @@ struct FusedInplaceCfg {
   static constexpr int ACC_WARPS = 8, CONV_WARPS = 6, CONV_WARP0 = 2 + ACC_WARPS;
   static constexpr int THREADS = (CONV_WARP0 + CONV_WARPS) * 32;
   static constexpr int MAX_REGS = 16384 / (32 * ((THREADS / 32 + 3) / 4)) / 8 * 8;
-  static constexpr int STAGING_PER_WARP = 32 * 32 * 4;  // one FP32 epilogue block per warp
+  static constexpr int STAGING_PER_WARP = STG * 32 * 32 * 4;
   static constexpr int STAGING_BYTES = ACC_WARPS * STAGING_PER_WARP;
   static constexpr int FIXED = 1024 + STAGING_BYTES + 512;
   static constexpr int NS_FIT = (kSmemBudget - FIXED) / STAGE;
@@ -440,11 +443,11 @@ __device__ __forceinline__ bool inplace_convert_b(uint8_t* stage, int c, Sync&& 
   return true;
 }
 
-template <class Tr>
-__global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
+template <class Tr, int STG>
+__global__ void __maxnreg__((FusedInplaceCfg<Tr, STG>::MAX_REGS))
     tc_fused_inplace_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                             const __grid_constant__ TcParams p) {
-  using F = FusedInplaceCfg<Tr>;
+  using F = FusedInplaceCfg<Tr, STG>;
   constexpr int BN = Tr::BN, NACC = Tr::NACC, NS = F::NS, NBUF = Tr::NBUF, TILE_M = Tr::TILE_M;
   constexpr int A_REGION = Tr::A_REGION;
 
@@ -461,8 +464,9 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
   uint64_t* drain = tempty + 4;
   uint64_t* conv_rd = drain + 1;  // this CTA's converters have read the stage's FP32 values
   uint64_t* fwd = conv_rd + 1;    // rank 1: this CTA's converters wrote the stage (forwarded to rank 0)
-  uint64_t* ebar = fwd + NS;      // one per promotion/epilogue warp: its TMA loads of C
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + F::ACC_WARPS);
+  uint64_t* ebar = fwd + NS;      // STG per promotion/epilogue warp: its TMA loads of C (one per staging block)
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(ebar + STG * F::ACC_WARPS);
+  static_assert((4 * NS + 10 + STG * F::ACC_WARPS) * 8 + 4 <= 512, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int units = p.tiles_m * p.tiles_n * p.splits;
@@ -483,7 +487,7 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
       mbar_init(&tempty[b], 2 * F::ACC_WARPS);
     }
     mbar_init(drain, 1);
-    for (int w = 0; w < F::ACC_WARPS; ++w) mbar_init(&ebar[w], 1);
+    for (int w = 0; w < STG * F::ACC_WARPS; ++w) mbar_init(&ebar[w], 1);
     fence_mbar_init();
   }
   if (warp == 1) {
@@ -617,8 +621,8 @@ __global__ void __maxnreg__((FusedInplaceCfg<Tr>::MAX_REGS))
       if (!ok) break;
       prefetch_unit(unit + unit_step);
       OutCtx o = out_ctx(p, u);
-      o.tbar = &ebar[warp - 2];
-      Tr::template finish<1>(o, master, stg, lane, row0, col0 + colsub, u.z);
+      o.tbar = &ebar[STG * (warp - 2)];  // the epilogue uses tbar[0 .. STG-1]
+      Tr::template finish<STG>(o, master, stg, lane, row0, col0 + colsub, u.z);
       ci += nchunks;
     }
     if (lane == 0) bulk_wait_all();  // this warp's TMA stores of C have completed
@@ -712,14 +716,14 @@ static cudaError_t launch_fused(const CUtensorMap& a, const CUtensorMap& b, cons
 }
 
 // a: A [128 rows][64 K] boxes, b: B [64 K][64 columns] boxes (no swizzle).
-template <class Tr>
+template <class Tr, int STG>
 static cudaError_t launch_fused_inplace(const CUtensorMap& a, const CUtensorMap& b, const TcParams& p, int sms,
                                         cudaStream_t st) {
-  using F = FusedInplaceCfg<Tr>;
+  using F = FusedInplaceCfg<Tr, STG>;
   static std::atomic<uint64_t> attr_set{0};
   static std::atomic<int> clusters_cached[64];
-  return launch_fused_kernel(tc_fused_inplace_kernel<Tr>, F::THREADS, F::SMEM, attr_set, clusters_cached, a, b, p, sms,
-                             st);
+  return launch_fused_kernel(tc_fused_inplace_kernel<Tr, STG>, F::THREADS, F::SMEM, attr_set, clusters_cached, a, b, p,
+                             sms, st);
 }
 
 }  // namespace tc
