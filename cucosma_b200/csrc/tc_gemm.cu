@@ -106,20 +106,17 @@ static Tiling make_tiling(const Plan& pl, int slices, int bn, const cucosma_gemm
 // GEMM's own bound (tensor time at nt products of BF16, or the HBM time of
 // reading the planes and writing -- with beta, also reading -- C): operands
 // read only a few times, as in the large-K and large-N families (measured on
-// B200, BF16x3, beta 0.5: 256 x 256 x 1,048,576 0.55 ms fused against about
-// 1.2 ms; 256 x 1,048,576 x 256 0.98 against 1.23 ms), and not where small
-// operands are re-read by many tiles (16384 x 16384 x 256: 0.89 fused against
-// 0.72 ms with the pre-pass, whose cost there is negligible).
+// B200, beta 0.5, BF16x3 / BF16x6: 256 x 256 x 1,048,576 0.58 / 0.88 ms fused
+// against about 1.2 / 2.6 ms; 256 x 1,048,576 x 256 0.85 / 1.06 against 1.23
+// / 1.19 ms), and not where small operands are re-read by many tiles (16384 x
+// 16384 x 256, BF16x6: 1.01 fused against 0.70 ms with the pre-pass, whose
+// cost there is negligible).
 static bool fused_pays(const cucosma_gemm_desc* d, int nt) {
   const double M = (double)d->m, N = (double)d->n, K = (double)d->k;
   const double hbm = 6.5e12, bf16 = 1.6e15;
   const double products = nt == 2 ? 3.0 : 6.0;
   const double c_bytes = M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0), ab_bytes = (M * K + K * N) * 4.0;
   if (ab_bytes < 32.0 * (1 << 20)) return false;  // small operands: the pre-pass costs microseconds
-  // BF16x6's fused kernel converts one k-block per stage and is slower than
-  // the pre-pass path where C dominates (256 x 1,048,576 x 256: 1.69 against
-  // 1.37 ms); the BF16x3 in-place kernel is faster there.
-  if (nt == 3 && c_bytes > 0.25 * ab_bytes) return false;
   const double t_pre = (M * K + K * N) * (4.0 + 2.0 * nt) / hbm;
   const double t_mma = 2.0 * M * N * K * products / bf16;
   const double t_mem = ((M * K + K * N) * 2.0 * nt + c_bytes) / hbm;
@@ -385,11 +382,10 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
     // FP32 operand tiles straight from the caller's buffers.  BF16x3 (in
     // place): A [128 rows][64 K] and B [64 K][64 columns] boxes, 256-byte
     // rows; BF16x6: A [128 rows][32 K] (128-byte swizzle) and B [32 K][64].
-    const bool inplace = pl.kind == 0;
-    const int kw = inplace ? 64 : 32;
+    const int kw = pl.kind == 0 ? 64 : 32;  // k-values per FP32 row of a stage
     CUtensorMap ta, tb;
     if (!encode_2d(&ta, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, d->lda, kw, 128,
-                   inplace ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B) ||
+                   pl.kind == 0 ? CU_TENSOR_MAP_SWIZZLE_NONE : CU_TENSOR_MAP_SWIZZLE_128B) ||
         !encode_2d(&tb, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, B, n, k, d->ldb, pl.bn_local, kw,
                    CU_TENSOR_MAP_SWIZZLE_NONE))
       return CUCOSMA_STATUS_LAUNCH_FAILED;
@@ -400,12 +396,13 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
     // (256 x 1,048,576 x 256, beta 0.5: 0.85 against 0.94 ms on B200)
     const double c_bytes = (double)d->m * d->n * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0);
     const double ab_bytes = ((double)d->m * d->k + (double)d->k * d->n) * 4.0;
-    if (!inplace)
-      e = launch_fused<Bf16x6Pair>(ta, tb, p, di->sms, st);
-    else if (c_bytes > 0.25 * ab_bytes)
-      e = launch_fused_inplace<Bf16x3Pair128, 2>(ta, tb, p, di->sms, st);
+    const bool c_heavy = c_bytes > 0.25 * ab_bytes;
+    if (pl.kind == 1)
+      e = c_heavy ? launch_fused_inplace<Bf16x6Pair, 2>(ta, tb, p, di->sms, st)
+                  : launch_fused_inplace<Bf16x6Pair, 1>(ta, tb, p, di->sms, st);
     else
-      e = launch_fused_inplace<Bf16x3Pair128, 1>(ta, tb, p, di->sms, st);
+      e = c_heavy ? launch_fused_inplace<Bf16x3Pair128, 2>(ta, tb, p, di->sms, st)
+                  : launch_fused_inplace<Bf16x3Pair128, 1>(ta, tb, p, di->sms, st);
     prof_end(st);
     launches += 1;
     if (e == cudaSuccess && pl.t.splits > 1) {
