@@ -45,17 +45,7 @@ enum Variant : int {
   kVOzaki = 7,
   kV3Fused = 10,     // BF16x3 256 x 128 pair, split fused into the kernel (tile id 5)
   kV6Fused = 11,     // BF16x6 256 x 128 pair, split fused into the kernel (tile id 4)
-  kV3PairC = 12,     // BF16x3 256 x 256 pair for C-heavy shapes: double-buffered 64-column C blocks (tile id 6)
 };
-
-// C traffic far above the operands' with a short K (the flat family): the
-// pair tile whose epilogue double-buffers 64-column C blocks (three stages
-// are enough for a few k-blocks a tile).
-static bool c_heavy_small_k(const cucosma_gemm_desc* d) {
-  const double M = (double)d->m, N = (double)d->n, K = (double)d->k;
-  const double c_bytes = M * N * 4.0 * (d->beta != 0.0 ? 2.0 : 1.0), ab_bytes = (M * K + K * N) * 4.0;
-  return K <= 1024 && c_bytes > 4.0 * ab_bytes;
-}
 
 // Tiling of one kernel: tiles, K blocks and splits, raster band.
 struct Tiling {
@@ -160,12 +150,8 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool all
         case 3: pl.variant = kV3Promoted; break;
         case 4: pl.variant = kV3Pair; break;
         case 5: pl.variant = allow_fused ? kV3Fused : kV3Pair; break;
-        case 6: pl.variant = kV3PairC; break;
         default:
-          pl.variant = !pair_ok                              ? kV3Promoted
-                       : (allow_fused && fused_pays(d, 2))   ? kV3Fused
-                       : c_heavy_small_k(d)                  ? kV3PairC
-                                                             : kV3Pair;
+          pl.variant = !pair_ok ? kV3Promoted : (allow_fused && fused_pays(d, 2)) ? kV3Fused : kV3Pair;
       }
     } else {
       switch (d->tile) {
@@ -184,10 +170,7 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool all
     pl.fused = pl.variant == kV3Fused || pl.variant == kV6Fused;
     pl.kpad = round_up(K, 8);
   }
-  pl.pair = (pl.variant == kV3Pair || pl.variant == kV3PairC || pl.variant == kV6Pair || pl.variant == kV6PairWide ||
-             pl.fused)
-                ? 1
-                : 0;
+  pl.pair = (pl.variant == kV3Pair || pl.variant == kV6Pair || pl.variant == kV6PairWide || pl.fused) ? 1 : 0;
   pl.tile_m = pl.pair ? 256 : 128;
   pl.bn_local = pl.pair ? bn / 2 : bn;
   pl.t = make_tiling(pl, slices, bn, d, di);
@@ -458,9 +441,6 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
       case kV3Small: e = launch<Bf16x3Promoted>(ta, tb, p, grid, st); break;
       case kV3Wide: e = launch<Bf16x3Wide>(ta, tb, p, grid, st); break;
       case kV3Pair: e = launch<Bf16x3Pair>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x3Pair>(di->sms)), st); break;
-      case kV3PairC:
-        e = launch<Bf16x3PairC>(ta, tb, p, pair_grid(max_pair_clusters<Bf16x3PairC>(di->sms)), st);
-        break;
       default: e = launch<Bf16x3>(ta, tb, p, grid, st);
     }
     prof_end(st);

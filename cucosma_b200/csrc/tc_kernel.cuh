@@ -557,16 +557,12 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
 // ------------------------------------------------------------ epilogues
 // FP32 result (BF16 split paths).  Each warp owns 32 rows; chunks of 32
 // columns go TMEM -> registers -> padded shared tile -> coalesced rows.
-// SB: 4 KB staging blocks per epilogue warp (2 by default; 4 for the tile
-// meant for C-heavy shapes, which double-buffers 64-column blocks).
-template <int SB>
-struct EpiF32T {
-  static constexpr bool kTmaStaging = true;
+struct EpiF32 {
   // A 32 x 32 FP32 block per warp: row r's 16-byte chunk c at c ^ (r & 7)
   // (the 128-byte swizzle TMA uses; the buffer is 1024-byte aligned).  Rows
   // are read and written as float4 chunks by the lane owning the row, and
   // columns one float per lane -- both free of bank conflicts.
-  static constexpr int STAGING_PER_WARP = SB * 32 * 32 * 4;
+  static constexpr int STAGING_PER_WARP = 2 * 32 * 32 * 4;  // two blocks: C loads overlap the previous block
   // Columns c0 .. c0 + 31 of a register accumulator row, as a 32-array (c0
   // is a compile-time constant at every use, so no copy is made).
   template <int BN>
@@ -820,54 +816,6 @@ struct EpiF32T {
     }
   }
 
-  // 64-column 3-D blocks, double-buffered (two 8 KB blocks): block i + 1's C
-  // load is in flight while block i is combined and stored.
-  template <int BN>
-  static __device__ __forceinline__ void finish_tma_wide2(const OutCtx& p, const float (&master)[BN], float* stg,
-                                                          int lane, int row0, int col0) {
-    const float alpha = (float)p.alpha, beta = (float)p.beta;
-    const bool ld = beta != 0.f;
-    constexpr int BLK = 2 * 32 * 32;  // floats in one 64-column block
-    if (lane == 0) bulk_wait_read_all();  // the previous tile's stores have read both blocks
-    __syncwarp();
-    uint64_t tok[2] = {0, 0};
-    if (ld && lane == 0 && col0 < p.n) {
-      tok[0] = mbar_arrive_expect_tx_token(&p.tbar[0], BLK * 4);
-      tma_load_3d(stg, p.tmc3, 0, col0 / 32, row0, &p.tbar[0]);
-    }
-#pragma unroll
-    for (int i = 0; i < BN / 64; ++i) {
-      const int col = col0 + 64 * i;
-      if (col >= p.n) break;
-      float* b = stg + (i & 1) * BLK;
-      if (ld) {
-        if (lane == 0 && !mbar_wait_token(&p.tbar[i & 1], tok[i & 1], kErrTimeoutOutput, p.ctl))
-          mbar_wait_token(&p.tbar[i & 1], tok[i & 1], kErrTimeoutDrain, p.ctl);
-        __syncwarp();
-      } else if (i >= 2) {
-        if (lane == 0) bulk_wait_read_but_last();  // the store from this block two steps ago has read it
-        __syncwarp();
-      }
-      float4* s4 = reinterpret_cast<float4*>(b);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int line = 2 * lane + h;
-        combine_row(p.epilogue, s4 + line * 8, cols32(master, 64 * i + 32 * h), alpha, beta, line);
-      }
-      fence_proxy_async_smem();  // the block is read by TMA (async proxy)
-      __syncwarp();
-      if (lane == 0) {
-        tma_store_3d(p.tmc3, b, 0, col / 32, row0);
-        bulk_commit();
-        if (ld && i + 1 < BN / 64 && col + 64 < p.n) {
-          bulk_wait_read_but_last();  // the other block's previous store has read it
-          tok[(i + 1) & 1] = mbar_arrive_expect_tx_token(&p.tbar[(i + 1) & 1], BLK * 4);
-          tma_load_3d(stg + ((i + 1) & 1) * BLK, p.tmc3, 0, (col + 64) / 32, row0, &p.tbar[(i + 1) & 1]);
-        }
-      }
-    }
-  }
-
   // STG: 32 x 32 staging blocks the warp has (2 in tc_gemm_kernel, 1 in the
   // fused kernels), fixed at compile time so only the matching paths exist.
   template <int BN, int STG>
@@ -875,13 +823,7 @@ struct EpiF32T {
                                                 int lane, int row0, int col0, int z) {
     float* stg = reinterpret_cast<float*>(stg_raw);
     if (p.tmc != nullptr) {
-      if constexpr (STG >= 4) {
-        if (p.tmc3 != nullptr && BN % 64 == 0)
-          finish_tma_wide2<BN>(p, master, stg, lane, row0, col0);
-        else
-          finish_tma2<BN>(p, master, stg, lane, row0, col0);
-        return;
-      } else if constexpr (STG >= 2) {
+      if constexpr (STG >= 2) {
         if (p.tmc3 != nullptr && BN % 64 == 0)
           finish_tma_wide<BN>(p, master, stg, lane, row0, col0);
         else
@@ -908,15 +850,12 @@ struct EpiF32T {
   }
 };
 
-using EpiF32 = EpiF32T<2>;
-
 // FP64 result (Ozaki).  Chunks of 16 columns: part = sum_{d = S-1..0}
 // S_d * 2^(-7(d+2)) (FP64, d descending), then 2^(e_row + e_col) and
 // alpha/beta; or the raw part into the split-K workspace.  Accumulator
 // layout: sub-tiles of SUB columns, each S diagonal blocks of SUB columns.
 template <int S, int SUB>
 struct EpiOzaki {
-  static constexpr bool kTmaStaging = false;
   static constexpr int STAGING_PER_WARP = 32 * 17 * 8;
   template <int BN>
   static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
@@ -1050,7 +989,7 @@ struct TraitsBase {
   static_assert(STAGES >= 2, "at least a double-buffered ring");
   static_assert(NACC * BN * NBUF <= 512, "accumulators exceed TMEM");
   static_assert(SMEM > 116 * 1024, "one CTA per SM keeps the 512-column TMEM allocation uncontended");
-  static_assert(!Epi::kTmaStaging || STAGE_BYTES % 1024 == 0,
+  static_assert(!std::is_same<Epi, EpiF32>::value || STAGE_BYTES % 1024 == 0,
                 "the FP32 epilogue's swizzled staging starts 1024-byte aligned");
   static_assert(!PROMOTE || (CHUNK > 0 && (NBUF >= 2 || SPLIT_)), "promotion needs chunk buffers");
   static_assert(!SPLIT_ || (PROMOTE_ && NACC_ == 2 && NBUF == 1), "split release: two accumulators, one buffer");
@@ -1125,11 +1064,6 @@ struct Bf16x6 : TraitsBase<6, 128, 64, 3, 3, 2, false, EpiF32, true, kPromoteChu
 //               (one buffer, split release); the 256 x 128 tiles need about
 //               1.5x the L2-to-shared-memory bandwidth per flop.
 struct Bf16x3Pair : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8, 0, true> {
-  static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
-};
-// The same pair tile for C-heavy shapes (small K, large C): four staging
-// blocks per epilogue warp (double-buffered 64-column C blocks), three stages.
-struct Bf16x3PairC : TraitsBase<3, 256, 64, 2, 2, 1, false, EpiF32T<4>, true, kPromoteChunk, 8, 0, true> {
   static constexpr TermTable<3> kTerms{{1, 0, 0}, {0, 1, 0}, {0, 0, 0}, {true, false, false}};
 };
 struct Bf16x3Pair128 : TraitsBase<3, 128, 64, 2, 2, 1, false, EpiF32, true, kPromoteChunk, 8, 0, true> {

@@ -83,15 +83,12 @@ typedef struct cucosma_gemm_desc {
                            *        2 = the 64 x 128 tile kernel (FP32; FP64 runs 128 x 128);
                            * BF16X3 1 = 128 x 256 without promotion, 2 = 128 x 128 promoted,
                            *        3 = 128 x 256 promoted, 4 = 256 x 256 CTA pair (default when m > 128),
-                           *        5 = 256 x 128 pair with the split fused in,
-                           *        6 = 256 x 256 pair with a double-buffered 64-column C epilogue;
+                           *        5 = 256 x 128 pair with the split fused in;
                            * BF16X6 1 = 128 x 128, 2 = 256 x 128 CTA pair,
                            *        3 = 256 x 256 CTA pair (default when m > 128),
                            *        4 = 256 x 128 pair with the split fused in.
                            * Auto (0) picks the fused kernels where the separate split pass
-                           * would cost more than a quarter of the GEMM (large K, large N),
-                           * and BF16X3 tile 6 where C traffic dwarfs the operands' with
-                           * K <= 1024 (flat shapes) */
+                           * would cost more than a quarter of the GEMM (large K, large N) */
   int32_t flags;          /* 0, or CUCOSMA_FLAG_TEST_SKIP_STAGE */
 } cucosma_gemm_desc;
 

@@ -63,13 +63,13 @@ def test_split_planes_bitexact(precision, nterms):
     assert np.array_equal(pb, oracle.split_bf16(np.ascontiguousarray(B.T), nterms))
 
 
-BF16_VARIANTS = [("bf16x3", 2, 0), ("bf16x3", 2, 1), ("bf16x3", 2, 2), ("bf16x3", 2, 3), ("bf16x3", 2, 6),
-                 ("bf16x6", 3, 0), ("bf16x6", 3, 1), ("bf16x6", 3, 2)]
+BF16_VARIANTS = [("bf16x3", 2, 0), ("bf16x3", 2, 1), ("bf16x3", 2, 2), ("bf16x3", 2, 3), ("bf16x6", 3, 0),
+                 ("bf16x6", 3, 1), ("bf16x6", 3, 2)]
 
 
 @pytest.mark.parametrize("precision,nterms,tile", BF16_VARIANTS,
                          ids=["bf16x3-pair256x256", "bf16x3-128x256wide", "bf16x3-128x128", "bf16x3-128x256",
-                              "bf16x3-pair256x256-c", "bf16x6-pair256x256", "bf16x6-128x128", "bf16x6-pair256x128"])
+                              "bf16x6-pair256x256", "bf16x6-128x128", "bf16x6-pair256x128"])
 @pytest.mark.parametrize("shape", SHAPES, ids=["%dx%dx%d" % s for s in SHAPES])
 def test_bf16_paths_vs_oracle(precision, nterms, tile, shape):
     m, n, k = shape
@@ -458,17 +458,3 @@ def test_sigmoid_epilogue_accuracy(precision):
     err = np.abs(out.astype(np.float64) - ref[:, None])
     ulp = np.spacing(ref.astype(np.float32)).astype(np.float64)[:, None]
     assert np.all((err <= 4 * ulp) | (err <= 1e-37)), float((err / ulp).max())
-
-
-def test_c_heavy_tile_bitexact():
-    """BF16x3 tile 6 (the pair tile whose epilogue double-buffers 64-column C
-    blocks) equals tile 4 bit for bit -- same products and promotion, only
-    the epilogue's staging differs -- on N a multiple of 32 (3-D boxes) and
-    not (2-D boxes), with beta and the sigmoid."""
-    for (m, n, k) in [(300, 320, 256), (513, 200, 96)]:
-        A = uniform(90, (m, k), lo=-0.5, hi=0.5)
-        B = uniform(91, (k, n), lo=-0.5, hi=0.5)
-        Cin = uniform(92, (m, n))
-        o6, p6 = run(A, B, Cin, 1.5, 0.5, "bf16x3", epilogue="sigmoid", tile=6)
-        o4, _ = run(A, B, Cin, 1.5, 0.5, "bf16x3", epilogue="sigmoid", tile=4)
-        assert p6["tile_m"] == 256 and np.array_equal(o6, o4)
