@@ -20,7 +20,9 @@ struct WaitCtl;
 void wait_ctl(const DeviceInfo* di, int** status, unsigned long long* timeout_ns);
 
 // Operand pre-passes of the tensor-core paths (see tc_gemm_ex).
-enum : int { kPrepA = 1, kPrepB = 2 };
+// kNoFused: never the fused-split kernel, even with both pre-passes (the
+// host-buffer call's row blocks share B's planes, which it does not write).
+enum : int { kPrepA = 1, kPrepB = 2, kNoFused = 4 };
 
 struct NativePlan {
   int bm;  // CTA tile rows: 128, or 64 (FP32 only); 128 columns either way

@@ -87,8 +87,11 @@ cucosma_status host_layout(const cucosma_gemm_desc* d, HostLayout* L) {
   L->lda = round_up(d->k, vec);
   L->ldb = round_up(d->n, vec);
   L->ldc = round_up(d->n, vec);
-  // Row blocks of at least 256 rows, at most kMaxBlocks of them.
-  L->blocks = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxBlocks / 2, d->m / 256));
+  // Row blocks of at least 512 rows (two 256-row pair tiles: a block still
+  // fills most of the SMs), at most kMaxBlocks of them.  More, smaller blocks
+  // shorten the tail after the last input copy (that block's GEMM and the
+  // copy-out of its C): 8192^3 BF16x6 went from 8 to 16 blocks.
+  L->blocks = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxBlocks, d->m / 512));
   L->rows_per_block = round_up(ceil_div(d->m, L->blocks), 128);
   L->blocks = (int)ceil_div(d->m, L->rows_per_block);
   // The regular entry point's workspace for a full row block and for the
@@ -105,6 +108,15 @@ cucosma_status host_layout(const cucosma_gemm_desc* d, HostLayout* L) {
     size_t b = 0;
     cucosma_status s = cucosma_gemm_workspace_size(&sub, &b);
     if (s != CUCOSMA_STATUS_SUCCESS) return s;
+    if (L->blocks > 1 && (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6)) {
+      // several row blocks run the pre-pass path (B's planes shared): its plan's workspace
+      const DeviceInfo* di = device_info();
+      if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
+      cucosma_gemm_desc tuned;
+      cucosma_plan_info pi;
+      tc_plan_info(apply_tuning(&sub, &tuned, di), di, &pi, false);
+      b = std::max(b, (size_t)pi.workspace_bytes);
+    }
     L->ws_bytes = std::max(L->ws_bytes, b);
   }
   size_t off = 0;
@@ -147,10 +159,13 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
   if (!h) return CUCOSMA_STATUS_LAUNCH_FAILED;
   CallEvents ev;
   if (!ev.create(L.blocks)) return CUCOSMA_STATUS_LAUNCH_FAILED;
-  // When the first block runs the fused-split kernel it writes no B planes,
-  // so the later blocks prepare their own.
+  // Several row blocks share B's planes, prepared by the first (the fused
+  // split, which keeps none, is not used then: per block it would read and
+  // split B again -- 512-row blocks of 8192^3 BF16x6 chose it and ran 12 %
+  // slower end to end).  A single block may take the fused kernel.
   bool b_shared = true;
-  if (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6) {
+  const int no_fused = L.blocks > 1 ? kNoFused : 0;
+  if (L.blocks == 1 && (d->precision == CUCOSMA_PRECISION_BF16X3 || d->precision == CUCOSMA_PRECISION_BF16X6)) {
     const DeviceInfo* di = device_info();
     if (!di) return CUCOSMA_STATUS_LAUNCH_FAILED;
     cucosma_gemm_desc first = *d;
@@ -198,7 +213,7 @@ extern "C" cucosma_status cucosma_gemm_host(const cucosma_gemm_desc* d, const vo
     sub.ldc = L.ldc;
     // B's operand planes: prepared by the first block, reused by the rest.
     s = gemm_ex(&sub, dA + r0 * L.lda * es, dB, dC + r0 * L.ldc * es, ws, L.ws_bytes, h->gemm,
-                (i == 0 || !b_shared) ? (kPrepA | kPrepB) : kPrepA);
+                ((i == 0 || !b_shared) ? (kPrepA | kPrepB) : kPrepA) | no_fused);
     if (s != CUCOSMA_STATUS_SUCCESS) return s;
     if (fail(cudaEventRecord(ev.c_ready[i], h->gemm)) || fail(cudaStreamWaitEvent(h->out, ev.c_ready[i], 0)) ||
         fail(cudaMemcpy2DAsync(hC + r0 * d->ldc * es, d->ldc * es, dC + r0 * L.ldc * es, L.ldc * es, d->n * es, rows,

@@ -370,7 +370,8 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
                           size_t ws_bytes, const DeviceInfo* di, cudaStream_t st, int prep) {
   // Callers that supply prepared planes (prep without both operands) never
   // get the fused kernel, which reads the FP32 operands themselves.
-  const bool allow_fused = prep == (kPrepA | kPrepB) && A != nullptr && B != nullptr;
+  const bool allow_fused =
+      (prep & (kPrepA | kPrepB)) == (kPrepA | kPrepB) && !(prep & kNoFused) && A != nullptr && B != nullptr;
   const Plan pl = make_plan(d, di, allow_fused);
   if (pl.bytes > 0 && (ws == nullptr || ws_bytes < pl.bytes)) return CUCOSMA_STATUS_WORKSPACE_TOO_SMALL;
   if (pl.kind == 2 && (pl.t.slices < 4 || pl.t.slices > 9)) return CUCOSMA_STATUS_NOT_SUPPORTED;
