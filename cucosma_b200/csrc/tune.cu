@@ -175,9 +175,12 @@ extern "C" cucosma_status cucosma_tune(const cucosma_gemm_desc* d, const void* A
   } else {
     bands = {8, 4, 16};
     // tensor-core tiles: BF16x3 128x128, 128x256, 256x256 (CTA pair);
-    // BF16x6 128x128, 256x128 (pair), 256x256 (pair); Ozaki one tile per slice count
-    if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = {2, 3, 4};
-    if (d->precision == CUCOSMA_PRECISION_BF16X6) tiles = {1, 2, 3};
+    // BF16x6 128x128, 256x128 (pair), 256x256 (pair); with operands of 32 MB
+    // or more also the fused-split pair (BF16x3 tile 5, BF16x6 tile 4); Ozaki
+    // one tile per slice count
+    const bool big = ((double)d->m * d->k + (double)d->k * d->n) * 4.0 >= 32.0 * (1 << 20) && d->flags == 0;
+    if (d->precision == CUCOSMA_PRECISION_BF16X3) tiles = big ? std::vector<int>{2, 3, 4, 5} : std::vector<int>{2, 3, 4};
+    if (d->precision == CUCOSMA_PRECISION_BF16X6) tiles = big ? std::vector<int>{1, 2, 3, 4} : std::vector<int>{1, 2, 3};
   }
   struct Cand {
     int sk, sw, ti;
