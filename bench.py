@@ -721,11 +721,13 @@ def shape_run(args):
     A = make_rect(m, k, 100, dt)
     B = make_rect(k, n, 101, dt)
     C = make_rect(m, n, 102, dt)
-    d = cc.make_desc(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue, tile=args.tile)
+    d = cc.make_desc(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue, tile=args.tile,
+                     swizzle=args.swizzle)
     ws = cc.alloc_workspace(d)
 
     def call():
-        cc.gemm(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue, workspace=ws, tile=args.tile)
+        cc.gemm(A, B, C, 1.0, args.beta, precision=prec, epilogue=args.epilogue, workspace=ws, tile=args.tile,
+                swizzle=args.swizzle)
 
     for _ in range(args.warmup):
         call()
@@ -766,6 +768,7 @@ def main():
     ap.add_argument("--beta", type=float, default=0.5)
     ap.add_argument("--epilogue", default="none")
     ap.add_argument("--tile", type=int, default=0, help="with --shape: tile id (0: the library's choice)")
+    ap.add_argument("--swizzle", type=int, default=0, help="with --shape: raster band (0: the library's choice)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
