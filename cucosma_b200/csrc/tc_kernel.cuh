@@ -787,6 +787,7 @@ struct EpiF32 {
                                                          int lane, int row0, int col0) {
     const float alpha = (float)p.alpha, beta = (float)p.beta;
     float4* s4 = reinterpret_cast<float4*>(stg);
+    const uint64_t pol = l2_evict_first_policy();
 #pragma unroll
     for (int i = 0; i < BN / 64; ++i) {
       const int col = col0 + 64 * i;
@@ -796,7 +797,7 @@ struct EpiF32 {
       if (beta != 0.f) {
         if (lane == 0) {
           const uint64_t token = mbar_arrive_expect_tx_token(&p.tbar[0], 2 * 32 * 32 * 4);
-          tma_load_3d(stg, p.tmc3, 0, col / 32, row0, &p.tbar[0]);
+          tma_load_3d_hint(stg, p.tmc3, 0, col / 32, row0, &p.tbar[0], pol);
           if (!mbar_wait_token(&p.tbar[0], token, kErrTimeoutOutput, p.ctl))
             mbar_wait_token(&p.tbar[0], token, kErrTimeoutDrain, p.ctl);
         }
@@ -810,7 +811,7 @@ struct EpiF32 {
       fence_proxy_async_smem();  // the block is read by TMA (async proxy)
       __syncwarp();
       if (lane == 0) {
-        tma_store_3d(p.tmc3, stg, 0, col / 32, row0);
+        tma_store_3d_hint(p.tmc3, stg, 0, col / 32, row0, pol);
         bulk_commit();
       }
     }
