@@ -295,7 +295,8 @@ bool measure_counters(const std::function<bool()>& run, cudaStream_t st, Counter
     ev.numMetrics = 3;
     ev.pMetricValues = values;
     if (c.evaluate(&ev) != CUPTI_SUCCESS) break;
-    out->l2_hit_pct = values[0];
+    // the counter ratio can read a few hundredths of a percent above 100
+    out->l2_hit_pct = values[0] < 0.0 ? 0.0 : (values[0] > 100.0 ? 100.0 : values[0]);
     out->dram_read_bytes = values[1];
     out->dram_write_bytes = values[2];
     ok = true;

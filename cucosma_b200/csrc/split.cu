@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(256)
 // stats->min_row by atomicMin (zero rows stay out).
 constexpr int kRowSteps = 8;                    // steps of 1024 columns held in registers
 constexpr int kRowRegK = kRowSteps * 1024;
+static_assert(kRowRegK == kOzakiRowChunk, "row chunk");
 
 __device__ __forceinline__ void load4(const double* __restrict__ src, int c, int cols, double (&v)[4]) {
   if (c + 4 <= cols) {
@@ -207,7 +208,8 @@ __device__ __forceinline__ void store_slices4(int8_t* __restrict__ out, int64_t 
 template <int S>
 __global__ void __launch_bounds__(256)
     ozaki_rows_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
-                      int32_t* __restrict__ ea, int8_t* __restrict__ out, OzakiStats* __restrict__ stats) {
+                      int32_t* __restrict__ ea, int8_t* __restrict__ out, unsigned long long* __restrict__ rowsum) {
+  const bool stats = rowsum != nullptr;
   __shared__ double red[8];
   __shared__ unsigned long long red_sum[8];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -278,7 +280,87 @@ __global__ void __launch_bounds__(256)
         unsigned long long t = 0;
 #pragma unroll
         for (int w = 0; w < 8; ++w) t += red_sum[w];
-        if (t > 0) atomicMin(&stats->min_row, t);
+        rowsum[r] = t;
+      }
+      __syncthreads();  // red_sum is reused by the next row
+    }
+  }
+}
+
+// Rows longer than kRowRegK in chunks of kRowRegK columns (grid.x chunks,
+// rows over grid.y), so that a few long rows still fill the GPU.  The first
+// kernel takes each chunk's maximum into ea[r] by atomicMax of its exponent
+// (ea starts at kExpSentinel; the exponent of a maximum is the maximum of
+// the exponents, so this is exact); the second cuts the chunk's slices and
+// adds its magnitude sum into rowsum[r] (integer atomics: exact and
+// independent of the order of the blocks).  Rows that are all zero keep the
+// sentinel until the second kernel's first chunk turns it into 0; every
+// block reads the sentinel as 0.
+__global__ void __launch_bounds__(256)
+    ozaki_row_exp_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int32_t* __restrict__ ea) {
+  __shared__ double red[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * kRowRegK;
+  for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+    const double* src = A + (int64_t)r * lda;
+    double m = 0.0;
+#pragma unroll
+    for (int j = 0; j < kRowSteps; ++j) {
+      const int c = c0 + (tid + 256 * j) * 4;
+      if (c < cols) {
+        double w[4];
+        load4(src, c, cols, w);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(w[q]));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) red[warp] = m;
+    __syncthreads();
+    m = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmax(m, red[w]);
+    __syncthreads();  // red is reused by the next row
+    if (tid == 0 && m != 0.0) atomicMax(&ea[r], exp_of(m));
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256)
+    ozaki_row_slice_kernel(const double* __restrict__ A, int64_t lda, int rows, int cols, int64_t kpad,
+                           int32_t* __restrict__ ea, int8_t* __restrict__ out, unsigned long long* __restrict__ rowsum) {
+  __shared__ unsigned long long red_sum[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int c0 = blockIdx.x * kRowRegK;
+  for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+    const double* src = A + (int64_t)r * lda;
+    int e = ea[r];
+    if (e == kExpSentinel) {
+      e = 0;
+      if (blockIdx.x == 0 && tid == 0) ea[r] = 0;
+    }
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int j = 0; j < kRowSteps; ++j) {
+      const int c = c0 + (tid + 256 * j) * 4;
+      if (c < kpad) {
+        double w[4];
+        load4(src, c, cols, w);
+        store_slices4<S>(out, r, c, kpad, w, e);
+        if (rowsum) sum += magnitude_fx4(w, e);
+      }
+    }
+    if (rowsum) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0) red_sum[warp] = sum;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += red_sum[w];
+        if (t) atomicAdd(&rowsum[r], t);
       }
       __syncthreads();  // red_sum is reused by the next row
     }
@@ -355,16 +437,15 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Minimum of the column magnitude sums over the nonzero columns into
-// stats->min_col; the last block to finish then makes the path choice (see
-// ozaki_choice) from both minima.
-__global__ void __launch_bounds__(256) ozaki_decide_kernel(const unsigned long long* __restrict__ colsum, int ncols,
-                                                           int64_t k, OzakiStats* stats) {
-  __shared__ unsigned long long red[8];
+// Minima of the row and column magnitude sums over the nonzero rows and
+// columns into stats->min_row / min_col; the last block to finish then
+// makes the path choice (see ozaki_choice) from both minima.
+__device__ __forceinline__ unsigned long long block_min_nonzero(const unsigned long long* __restrict__ v, int count,
+                                                                unsigned long long* red) {
   unsigned long long m = ~0ull;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ncols; i += gridDim.x * blockDim.x) {
-    const unsigned long long v = colsum[i];
-    if (v != 0 && v < m) m = v;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const unsigned long long x = v[i];
+    if (x != 0 && x < m) m = x;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -373,8 +454,19 @@ __global__ void __launch_bounds__(256) ozaki_decide_kernel(const unsigned long l
   }
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
+  for (int w = 0; w < 8; ++w) m = red[w] < m ? red[w] : m;
+  __syncthreads();  // red is reused
+  return m;
+}
+
+__global__ void __launch_bounds__(256) ozaki_decide_kernel(const unsigned long long* __restrict__ rowsum, int nrows,
+                                                           const unsigned long long* __restrict__ colsum, int ncols,
+                                                           int64_t k, OzakiStats* stats) {
+  __shared__ unsigned long long red[8];
+  const unsigned long long mrow = block_min_nonzero(rowsum, nrows, red);
+  const unsigned long long m = block_min_nonzero(colsum, ncols, red);
   if (threadIdx.x == 0) {
-    for (int w = 0; w < 8; ++w) m = red[w] < m ? red[w] : m;
+    if (mrow != ~0ull) atomicMin(&stats->min_row, mrow);
     if (m != ~0ull) atomicMin(&stats->min_col, m);
     __threadfence();
     const unsigned prev = atomicAdd(&stats->done_blocks, 1u);
@@ -440,9 +532,19 @@ static cudaError_t prep_b_s(const double* B, int64_t ldb, int k, int n, int64_t 
 
 template <int S>
 static cudaError_t prep_a_s(const double* A, int64_t lda, int m, int k, int64_t kpad, int32_t* ea, int8_t* sa,
-                            OzakiStats* stats, int sms, cudaStream_t st) {
-  const unsigned rows_grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(m, (int64_t)sms * 8));
-  ozaki_rows_kernel<S><<<rows_grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, stats);
+                            unsigned long long* rowsum, int sms, cudaStream_t st) {
+  if (kpad <= kRowRegK) {
+    const unsigned rows_grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(m, (int64_t)sms * 8));
+    ozaki_rows_kernel<S><<<rows_grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, rowsum);
+    return cudaGetLastError();
+  }
+  cudaError_t e = cudaMemsetAsync(ea, 0x80, (size_t)m * sizeof(int32_t), st);
+  if (e == cudaSuccess && rowsum) e = cudaMemsetAsync(rowsum, 0, (size_t)m * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)ceil_div(kpad, kRowRegK), (unsigned)std::min<int64_t>(m, 65535));
+  ozaki_row_exp_kernel<<<grid, 256, 0, st>>>(A, lda, m, k, ea);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  ozaki_row_slice_kernel<S><<<grid, 256, 0, st>>>(A, lda, m, k, kpad, ea, sa, rowsum);
   return cudaGetLastError();
 }
 
@@ -470,7 +572,7 @@ cudaError_t launch_ozaki_prep_b(int s, const double* B, int64_t ldb, int k, int 
 }
 
 cudaError_t launch_ozaki_prep_a(int s, const double* A, int64_t lda, int m, int k, int64_t kpad, int32_t* ea,
-                                int8_t* sa, OzakiStats* stats, int sms, cudaStream_t st) {
+                                int8_t* sa, unsigned long long* rowsum, OzakiStats* stats, int sms, cudaStream_t st) {
   if (stats) {
     // min_row, done_blocks and choice restart for every A (min_col belongs to B)
     cudaError_t e = cudaMemsetAsync(&stats->min_row, 0xFF, sizeof(stats->min_row), st);
@@ -479,20 +581,21 @@ cudaError_t launch_ozaki_prep_a(int s, const double* A, int64_t lda, int m, int 
     if (e != cudaSuccess) return e;
   }
   switch (s) {
-    case 4: return prep_a_s<4>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
-    case 5: return prep_a_s<5>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
-    case 6: return prep_a_s<6>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
-    case 7: return prep_a_s<7>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
-    case 8: return prep_a_s<8>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
-    case 9: return prep_a_s<9>(A, lda, m, k, kpad, ea, sa, stats, sms, st);
+    case 4: return prep_a_s<4>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
+    case 5: return prep_a_s<5>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
+    case 6: return prep_a_s<6>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
+    case 7: return prep_a_s<7>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
+    case 8: return prep_a_s<8>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
+    case 9: return prep_a_s<9>(A, lda, m, k, kpad, ea, sa, stats ? rowsum : nullptr, sms, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_ozaki_decide(const unsigned long long* colsum, int n, int64_t k, OzakiStats* stats, int sms,
-                                cudaStream_t st) {
-  const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 2));
-  ozaki_decide_kernel<<<blocks, 256, 0, st>>>(colsum, n, k, stats);
+cudaError_t launch_ozaki_decide(const unsigned long long* rowsum, int m, const unsigned long long* colsum, int n,
+                                int64_t k, OzakiStats* stats, int sms, cudaStream_t st) {
+  const unsigned blocks =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(std::max(m, n), 256), (int64_t)sms * 2));
+  ozaki_decide_kernel<<<blocks, 256, 0, st>>>(rowsum, m, colsum, n, k, stats);
   return cudaGetLastError();
 }
 

@@ -58,6 +58,10 @@ __host__ __device__ inline int ozaki_choice(unsigned long long min_row, unsigned
   return 0;
 }
 constexpr int kOzakiLayoutAdaptive = 9;  // slices produced when the count is chosen on the device
+// Rows of A longer than this (in padded columns) are prepared in chunks of
+// this many columns by two kernels (exponents, then slices); shorter rows by
+// one kernel that holds the row in registers.
+constexpr int kOzakiRowChunk = 8192;
 
 // B (k x n) -> per-column exponents eb (|b_kn| < 2^eb_n, 0 for zero columns)
 // and s INT8 slices of the columns, stacked: byte (n, k, p) at
@@ -69,13 +73,14 @@ cudaError_t launch_ozaki_prep_b(int s, const double* B, int64_t ldb, int k, int 
 // A (m x k) -> row exponents ea and s INT8 slices of the rows, packed (four
 // slices' 32-byte k-blocks per 128-byte row): byte (r, k, p) at
 // r * kpad * s + (k / 32) * 32 * s + p * 32 + k % 32; kpad a multiple of 32.
-// With stats, also the smallest row magnitude sum (stats->min_row; the
-// decision fields are reset first).
+// With stats, also the rows' magnitude sums into rowsum (m entries; the
+// decision fields of stats are reset first).
 cudaError_t launch_ozaki_prep_a(int s, const double* A, int64_t lda, int m, int k, int64_t kpad, int32_t* ea,
-                                int8_t* sa, OzakiStats* stats, int sms, cudaStream_t st);
+                                int8_t* sa, unsigned long long* rowsum, OzakiStats* stats, int sms, cudaStream_t st);
 
-// After both preparations: stats->min_col from colsum, then stats->choice.
-cudaError_t launch_ozaki_decide(const unsigned long long* colsum, int n, int64_t k, OzakiStats* stats, int sms,
-                                cudaStream_t st);
+// After both preparations: stats->min_row / min_col from rowsum and colsum,
+// then stats->choice.
+cudaError_t launch_ozaki_decide(const unsigned long long* rowsum, int m, const unsigned long long* colsum, int n,
+                                int64_t k, OzakiStats* stats, int sms, cudaStream_t st);
 
 }  // namespace cucosma

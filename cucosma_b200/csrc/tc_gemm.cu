@@ -65,7 +65,7 @@ struct Plan {
   // Workspace: operand B first (its planes / slices, exponents and
   // magnitude sums depend on N and K only, so row blocks of one problem can
   // share them), then A, then the split-K partials of whichever kernel runs.
-  size_t off_b, off_eb, off_colsum, off_stats, off_a, off_ea, off_part, bytes;
+  size_t off_b, off_eb, off_colsum, off_stats, off_a, off_ea, off_rowsum, off_part, bytes;
   int64_t ldw;
 };
 
@@ -200,8 +200,12 @@ static Plan make_plan(const cucosma_gemm_desc* d, const DeviceInfo* di, bool all
   }
   pl.off_a = off;
   off = al256(off + ls * M * pl.kpad * es_in);
-  pl.off_ea = off;
-  if (pl.kind == 2) off = al256(off + (size_t)M * 4);
+  pl.off_ea = pl.off_rowsum = off;
+  if (pl.kind == 2) {
+    off = al256(off + (size_t)M * 4);
+    pl.off_rowsum = off;
+    if (pl.adaptive) off = al256(off + (size_t)M * 8);
+  }
   pl.ldw = round_up(N, 4);
   pl.off_part = off;
   size_t part = pl.t.splits > 1 ? (size_t)pl.t.splits * M * pl.ldw * es_out : 0;
@@ -457,6 +461,7 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
     int32_t* eb = reinterpret_cast<int32_t*>(w + pl.off_eb);
     OzakiStats* stats = pl.adaptive ? reinterpret_cast<OzakiStats*>(w + pl.off_stats) : nullptr;
     unsigned long long* colsum = pl.adaptive ? reinterpret_cast<unsigned long long*>(w + pl.off_colsum) : nullptr;
+    unsigned long long* rowsum = pl.adaptive ? reinterpret_cast<unsigned long long*>(w + pl.off_rowsum) : nullptr;
     if (prep & kPrepB) {
       e = launch_ozaki_prep_b(ls, (const double*)B, d->ldb, k, n, pl.kpad, eb, reinterpret_cast<int8_t*>(w + pl.off_b),
                               colsum, stats, di->sms, st);
@@ -464,11 +469,11 @@ cucosma_status tc_gemm_ex(const cucosma_gemm_desc* d, const void* A, const void*
     }
     if (e == cudaSuccess && (prep & kPrepA)) {
       e = launch_ozaki_prep_a(ls, (const double*)A, d->lda, m, k, pl.kpad, ea, reinterpret_cast<int8_t*>(w + pl.off_a),
-                              stats, di->sms, st);
-      launches += 1;
+                              rowsum, stats, di->sms, st);
+      launches += pl.kpad > kOzakiRowChunk ? 2 : 1;  // long rows: exponent and slicing kernels
     }
     if (e == cudaSuccess && pl.adaptive) {
-      e = launch_ozaki_decide(colsum, n, k, stats, di->sms, st);
+      e = launch_ozaki_decide(rowsum, m, colsum, n, k, stats, di->sms, st);
       launches += 1;
     }
     if (e != cudaSuccess) return CUCOSMA_STATUS_LAUNCH_FAILED;

@@ -531,8 +531,14 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
         if (!ok) break;
         tc_fence_after();
         prefetch_unit(unit + unit_step);
-        Tr::epilogue(octx(), lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
-        release(buf);
+        if constexpr (Tr::kDrain) {
+          Tr::drain(lane_base + (uint32_t)(buf * NACC * BN), stg, lane);
+          release(buf);  // the next unit's MMAs run during the stores below
+          Tr::store(octx(), stg, lane, row0, col0, z);
+        } else {
+          Tr::epilogue(octx(), lane_base + (uint32_t)(buf * NACC * BN), stg, lane, row0, col0, z);
+          release(buf);
+        }
         ++ci;
       }
     }
@@ -558,6 +564,7 @@ __global__ void __maxnreg__(Tr::MAX_REGS)
 // FP32 result (BF16 split paths).  Each warp owns 32 rows; chunks of 32
 // columns go TMEM -> registers -> padded shared tile -> coalesced rows.
 struct EpiF32 {
+  static constexpr bool kDrain = false;
   // A 32 x 32 FP32 block per warp: row r's 16-byte chunk c at c ^ (r & 7)
   // (the 128-byte swizzle TMA uses; the buffer is 1024-byte aligned).  Rows
   // are read and written as float4 chunks by the lane owning the row, and
@@ -857,61 +864,115 @@ struct EpiF32 {
 // layout: sub-tiles of SUB columns, each S diagonal blocks of SUB columns.
 template <int S, int SUB>
 struct EpiOzaki {
-  static constexpr int STAGING_PER_WARP = 32 * 17 * 8;
+  // Two-phase form (kDrain): the warp first drains its 32 rows x BN of the
+  // accumulator into a padded shared tile (LD doubles a row) and releases
+  // TMEM, so that the next unit's MMAs overlap the C combine and stores.  The
+  // accumulator fills all 512 TMEM columns (one buffer), so without this the
+  // MMA warp waits for the whole epilogue.  S = 5 and 9 keep the one-phase
+  // form: their stages are larger and the tile would leave two ring stages.
+  static constexpr bool kDrain = S != 5 && S != 9;
+  static constexpr int LD = ozaki_bn(S) + 1;  // (LD * 2) % 32 == 2: conflict-free row writes
+  static constexpr int STAGING_PER_WARP = kDrain ? 32 * LD * 8 : 32 * 17 * 8;
+
+  // part[j] = sum_d S_d 2^(-7(d+2)) for this lane's row at column c0 + j of
+  // the tile, d descending; two diagonals' TMEM loads share one wait.
+  static __device__ __forceinline__ void recombine(uint32_t tacc, int c0, double (&part)[16]) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) part[j] = 0.0;
+    const uint32_t base = tacc + (uint32_t)((c0 / SUB) * S * SUB + c0 % SUB);
+#pragma unroll
+    for (int d = S - 1; d >= 0; d -= 2) {
+      uint32_t v[16], u[16];
+      tmem_ld16(base + (uint32_t)(d * SUB), v);
+      if (d >= 1) tmem_ld16(base + (uint32_t)((d - 1) * SUB), u);
+      tmem_ld_wait();
+      const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+      for (int j = 0; j < 16; ++j) part[j] = part[j] + (double)(int32_t)v[j] * w;
+      if (d >= 1) {
+        const double w1 = ldexp(1.0, -7 * (d + 1));
+#pragma unroll
+        for (int j = 0; j < 16; ++j) part[j] = part[j] + (double)(int32_t)u[j] * w1;
+      }
+    }
+  }
+
+  // One 16-column block of results: lane (cl = lane % 16, rows (lane >> 4) + 2h)
+  // takes its 16 values from the shared tile at stg[r * ld + cl] and writes
+  // them (scaled by 2^(e_row + e_col), alpha / beta, activation) or, for a
+  // split-K unit, the raw parts into the workspace.
+  static __device__ __forceinline__ void store_block(const OutCtx& p, const double* stg, int ld, int lane, int row0,
+                                                     int col, int z) {
+    if (col >= p.n) return;
+    const int ecol = p.partial ? 0 : p.eb[col];
+    // This lane's row exponents and, when beta != 0, its C values, read
+    // together up front (the stores below may alias them, so they are not
+    // reordered otherwise): one read latency a block instead of one a row.
+    int erow[16];
+    double cv[16];
+#pragma unroll
+    for (int h = 0; h < 16; ++h) {
+      const int row = row0 + (lane >> 4) + 2 * h;
+      const bool in = !p.partial && row < p.m;
+      erow[h] = in ? p.ea[row] : 0;
+      cv[h] = in && p.beta != 0.0 ? reinterpret_cast<const double*>(p.out)[(int64_t)row * p.ldo + col] : 0.0;
+    }
+#pragma unroll
+    for (int h = 0; h < 16; ++h) {
+      const int r = (lane >> 4) + 2 * h;
+      const int row = row0 + r;
+      if (row >= p.m) continue;
+      const double v = stg[r * ld + (lane & 15)];
+      if (p.partial) {
+        reinterpret_cast<double*>(p.out)[(int64_t)z * p.ws_split_stride + (int64_t)row * p.ldo + col] = v;
+      } else {
+        double* po = reinterpret_cast<double*>(p.out) + (int64_t)row * p.ldo + col;
+        const double r_ = ldexp(v, erow[h] + ecol);
+        const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * cv[h]);
+        *po = apply_epi(o, p.epilogue);
+      }
+    }
+  }
+
+  // Phase 1 of the two-phase form: TMEM -> shared tile (row lane, LD doubles a row).
+  template <int BN>
+  static __device__ __forceinline__ void drain(uint32_t tacc, uint8_t* stg_raw, int lane) {
+    static_assert(!kDrain || BN + 1 == LD, "tile width");
+    double* row = reinterpret_cast<double*>(stg_raw) + lane * LD;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      double part[16];
+      recombine(tacc, c0, part);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) row[c0 + j] = part[j];
+    }
+    __syncwarp();
+  }
+
+  // Phase 2: shared tile -> C (or the split-K workspace).
+  template <int BN>
+  static __device__ __forceinline__ void store(const OutCtx& p, const uint8_t* stg_raw, int lane, int row0, int col0,
+                                               int z) {
+    const double* stg = reinterpret_cast<const double*>(stg_raw);
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN && col0 + c0 < p.n; c0 += 16)
+      store_block(p, stg + c0, LD, lane, row0, col0 + c0 + (lane & 15), z);
+    __syncwarp();  // the next unit's drain overwrites the tile
+  }
+
+  // One-phase form: per 16-column block, TMEM -> padded 32 x 17 block -> C.
   template <int BN>
   static __device__ __forceinline__ void run(const OutCtx& p, uint32_t tacc, uint8_t* stg_raw, int lane, int row0,
                                              int col0, int z) {
     double* stg = reinterpret_cast<double*>(stg_raw);
-    const int cl = lane & 15;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
-      const int col = col0 + c0 + cl;
       double part[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) part[j] = 0.0;
-#pragma unroll
-      for (int d = S - 1; d >= 0; --d) {
-        uint32_t v[16];
-        tmem_ld16(tacc + (uint32_t)((c0 / SUB) * S * SUB + d * SUB + c0 % SUB), v);
-        tmem_ld_wait();
-        const double w = ldexp(1.0, -7 * (d + 2));
-#pragma unroll
-        for (int j = 0; j < 16; ++j) part[j] = part[j] + (double)(int32_t)v[j] * w;
-      }
+      recombine(tacc, c0, part);
 #pragma unroll
       for (int j = 0; j < 16; ++j) stg[lane * 17 + j] = part[j];
       __syncwarp();
-      if (col < p.n) {
-        const int ecol = p.partial ? 0 : p.eb[col];
-        // This lane's 16 outputs (column col, rows (lane >> 4) + 2h): their row
-        // exponents and, when beta != 0, their C values, read together up
-        // front (the stores below may alias them, so they are not reordered
-        // otherwise): one read latency a chunk instead of one a row.
-        int erow[16];
-        double cv[16];
-#pragma unroll
-        for (int h = 0; h < 16; ++h) {
-          const int row = row0 + (lane >> 4) + 2 * h;
-          const bool in = !p.partial && row < p.m;
-          erow[h] = in ? p.ea[row] : 0;
-          cv[h] = in && p.beta != 0.0 ? reinterpret_cast<const double*>(p.out)[(int64_t)row * p.ldo + col] : 0.0;
-        }
-#pragma unroll
-        for (int h = 0; h < 16; ++h) {
-          const int r = (lane >> 4) + 2 * h;
-          const int row = row0 + r;
-          if (row >= p.m) continue;
-          const double v = stg[r * 17 + cl];
-          if (p.partial) {
-            reinterpret_cast<double*>(p.out)[(int64_t)z * p.ws_split_stride + (int64_t)row * p.ldo + col] = v;
-          } else {
-            double* po = reinterpret_cast<double*>(p.out) + (int64_t)row * p.ldo + col;
-            const double r_ = ldexp(v, erow[h] + ecol);
-            const double o = p.beta == 0.0 ? p.alpha * r_ : fma(p.alpha, r_, p.beta * cv[h]);
-            *po = apply_epi(o, p.epilogue);
-          }
-        }
-      }
+      store_block(p, stg, 17, lane, row0, col0 + c0 + (lane & 15), z);
       __syncwarp();
     }
   }
@@ -997,6 +1058,14 @@ struct TraitsBase {
   static __device__ __forceinline__ void epilogue(const OutCtx& p, uint32_t tacc, uint8_t* stg, int lane, int row0,
                                                   int col0, int z) {
     Epi::template run<BN>(p, tacc, stg, lane, row0, col0, z);
+  }
+  static constexpr bool kDrain = Epi::kDrain;
+  static __device__ __forceinline__ void drain(uint32_t tacc, uint8_t* stg, int lane) {
+    Epi::template drain<BN>(tacc, stg, lane);
+  }
+  static __device__ __forceinline__ void store(const OutCtx& p, const uint8_t* stg, int lane, int row0, int col0,
+                                               int z) {
+    Epi::template store<BN>(p, stg, lane, row0, col0, z);
   }
   static __device__ __forceinline__ void accumulate(uint32_t tacc, float (&master)[COLS_PER_EW]) {
     if constexpr (PROMOTE) Epi::template accumulate<COLS_PER_EW, BN, NACC>(tacc, master);

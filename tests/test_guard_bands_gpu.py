@@ -29,6 +29,8 @@ CASES = [  # (precision, dtype, m, n, k, split_k[, tile])
     ("bf16x3", np.float32, 300, 132, 3000, 0, 5), ("bf16x6", np.float32, 300, 132, 3000, 0, 4),
     # N a multiple of 32 with an odd number of 32-column chunks: 64-column 3-D boxes, the last half outside
     ("bf16x3", np.float32, 129, 96, 65, 0), ("bf16x6", np.float32, 260, 160, 45, 0),
+    # FP64 with N even: the Ozaki results leave through 32 x 16 TMA boxes
+    ("ozaki", np.float64, 129, 66, 33, 0), ("ozaki", np.float64, 300, 130, 700, 0),
 ]
 
 

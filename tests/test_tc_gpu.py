@@ -164,7 +164,7 @@ def test_ozaki_slices_bitexact(dist):
 OZ_SHAPES = [(1, 1, 1), (7, 5, 3), (128, 64, 32), (129, 65, 33), (300, 200, 100), (256, 256, 1024), (1000, 48, 77)]
 
 
-@pytest.mark.parametrize("s", [6, 7, 8, 9])
+@pytest.mark.parametrize("s", [4, 5, 6, 7, 8, 9])
 @pytest.mark.parametrize("shape", OZ_SHAPES, ids=["%dx%dx%d" % x for x in OZ_SHAPES])
 def test_ozaki_bitexact_vs_restatement(shape, s):
     m, n, k = shape
@@ -330,6 +330,31 @@ def test_ozaki_default_uniform_chooses_8_slices_bitexact():
     assert _choice(ws, plan) == 8 == oracle.ozaki_choice(A, B)
     kchunk = plan["kchunk"] if plan["splits"] > 1 else 0
     assert np.array_equal(out, oracle.ozaki_gemm(A, B, 8, Cin=Cin, alpha=1.0, beta=0.5, kchunk=kchunk))
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_ozaki_long_rows_bitexact(adaptive):
+    """Rows of A longer than 8192 padded columns are prepared in 8192-column
+    chunks: an exponent kernel (chunk maxima by atomicMax) and a slicing
+    kernel (chunk magnitude sums added into per-row totals).  Row exponents,
+    the device's choice (from the row and column sums) and the result are
+    bit-exact against the restatement; one row is zero and one has its
+    maximum in the last, partial chunk."""
+    m, n, k = 40, 24, 20000
+    A = uniform(70, (m, k), np.float64) * 1e-3
+    A[3, :] = 0.0
+    A[7, 19000] = 0.01
+    B = uniform(71, (k, n), np.float64)
+    Cin = uniform(72, (m, n), np.float64)
+    out, plan, ws = run(A, B, Cin, 1.0, 0.5, "ozaki", slices=0 if adaptive else 8, keep_ws=True)
+    ea, _, _, _ = oracle.ozaki_slices(A, B, 8)
+    assert np.array_equal(ws[plan["off_ea"]: plan["off_ea"] + 4 * m].view(np.int32), ea)
+    s = 8
+    if adaptive:
+        s = _choice(ws, plan)
+        assert s == oracle.ozaki_choice(A, B) and s in (8, 9)
+    kchunk = plan["kchunk"] if plan["splits"] > 1 else 0
+    assert np.array_equal(out, oracle.ozaki_gemm(A, B, s, Cin=Cin, alpha=1.0, beta=0.5, kchunk=kchunk))
 
 
 def test_ozaki_default_spread_falls_back_to_native_fp64():
