@@ -205,15 +205,10 @@ __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEnt
 #pragma unroll
         for (int j = 0; j < 4; ++j) v[j] = c + j < e.k ? src[c + j] : 0.0;
       }
-      int8_t q[4][S];
+      uint32_t w[S];
+      slice4_packed<S>(v, ex, w);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) slice_value<S>(v[j], ex, q[j]);
-#pragma unroll
-      for (int t = 0; t < S; ++t) {
-        const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
-                            ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
-        *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, e.kpad, t)) = pk;
-      }
+      for (int t = 0; t < S; ++t) *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, e.kpad, t)) = w[t];
     }
     return;
   }
@@ -252,15 +247,11 @@ __global__ void __launch_bounds__(256) grouped_ozaki_slice_kernel(const GroupEnt
     const int n = n0 + nl, k = k0 + kq * 4;
     if (n >= e.n) continue;
     const int ex = e.eb[n];
-    int8_t q[4][S];
+    const double v[4] = {tile[kq * 4][nl], tile[kq * 4 + 1][nl], tile[kq * 4 + 2][nl], tile[kq * 4 + 3][nl]};
+    uint32_t w[S];
+    slice4_packed<S>(v, ex, w);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) slice_value<S>(tile[kq * 4 + j][nl], ex, q[j]);
-#pragma unroll
-    for (int s_ = 0; s_ < S; ++s_) {
-      const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
-                          ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
-      *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, e.n, s_)) = pk;
-    }
+    for (int s_ = 0; s_ < S; ++s_) *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, e.n, s_)) = w[s_];
   }
 }
 

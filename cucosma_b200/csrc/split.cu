@@ -191,18 +191,16 @@ __device__ __forceinline__ void load4(const double* __restrict__ src, int c, int
   }
 }
 
+// Slices of 4 consecutive columns of row r (one 4-byte store per slice);
+// returns their magnitude sum (see slice4_packed).
 template <int S>
-__device__ __forceinline__ void store_slices4(int8_t* __restrict__ out, int64_t r, int c, int64_t kpad,
-                                              const double (&v)[4], int e) {
-  int8_t q[4][S];
+__device__ __forceinline__ unsigned long long store_slices4(int8_t* __restrict__ out, int64_t r, int c, int64_t kpad,
+                                                            const double (&v)[4], int e) {
+  uint32_t w[S];
+  const unsigned long long mag = slice4_packed<S>(v, e, w);
 #pragma unroll
-  for (int j = 0; j < 4; ++j) slice_value<S>(v[j], e, q[j]);
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const uint32_t pk = (uint32_t)(uint8_t)q[0][t] | ((uint32_t)(uint8_t)q[1][t] << 8) |
-                        ((uint32_t)(uint8_t)q[2][t] << 16) | ((uint32_t)(uint8_t)q[3][t] << 24);
-    *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, kpad, t)) = pk;
-  }
+  for (int t = 0; t < S; ++t) *reinterpret_cast<uint32_t*>(out + packed_index<S>(r, c, kpad, t)) = w[t];
+  return mag;
 }
 
 template <int S>
@@ -258,8 +256,8 @@ __global__ void __launch_bounds__(256)
       for (int j = 0; j < kRowSteps; ++j) {
         const int c = (tid + 256 * j) * 4;
         if (c < kpad) {
-          store_slices4<S>(out, r, c, kpad, v[j], e);
-          if (stats) sum += magnitude_fx4(v[j], e);
+          const unsigned long long mg = store_slices4<S>(out, r, c, kpad, v[j], e);
+          if (stats) sum += mg;
         }
       }
     } else {
@@ -267,8 +265,8 @@ __global__ void __launch_bounds__(256)
       for (int c = tid * 4; c < kpad; c += 1024) {
         double w[4];
         load4(src, c, cols, w);
-        store_slices4<S>(out, r, c, kpad, w, e);
-        if (stats) sum += magnitude_fx4(w, e);
+        const unsigned long long mg = store_slices4<S>(out, r, c, kpad, w, e);
+        if (stats) sum += mg;
       }
     }
     if (stats) {
@@ -347,8 +345,8 @@ __global__ void __launch_bounds__(256)
       if (c < kpad) {
         double w[4];
         load4(src, c, cols, w);
-        store_slices4<S>(out, r, c, kpad, w, e);
-        if (rowsum) sum += magnitude_fx4(w, e);
+        const unsigned long long mg = store_slices4<S>(out, r, c, kpad, w, e);
+        if (rowsum) sum += mg;
       }
     }
     if (rowsum) {
@@ -417,16 +415,11 @@ __global__ void __launch_bounds__(256)
       double v[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) v[j] = tile[kq * 4 + j][nl];
-      int8_t q[4][S];
+      uint32_t w[S];
+      const unsigned long long mg = slice4_packed<S>(v, e, w);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) slice_value<S>(v[j], e, q[j]);
-#pragma unroll
-      for (int s_ = 0; s_ < S; ++s_) {
-        const uint32_t pk = (uint32_t)(uint8_t)q[0][s_] | ((uint32_t)(uint8_t)q[1][s_] << 8) |
-                            ((uint32_t)(uint8_t)q[2][s_] << 16) | ((uint32_t)(uint8_t)q[3][s_] << 24);
-        *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, ncols, s_)) = pk;
-      }
-      if (colsum) part = magnitude_fx4(v, e);
+      for (int s_ = 0; s_ < S; ++s_) *reinterpret_cast<uint32_t*>(out + stacked_index<S>(n, k, ncols, s_)) = w[s_];
+      if (colsum) part = mg;
     }
     if (colsum) {
       // the 8 lanes of a column are consecutive: reduce over them

@@ -68,26 +68,19 @@ __device__ __forceinline__ int exp_of(double amax) {
 // |v| = M * 2^(E - 1075) with the 53-bit significand M (E the biased
 // exponent; M without the hidden bit and E = 1 for subnormals), so the
 // first 7 S bits F = floor(|v| * 2^(7 S - e)) = M shifted by
-// 7 S - e + E - 1075 (right when negative).
+// 7 S - e + E - 1075 (right when negative); q_t = +-((F >> 7 (S - 1 - t)) & 127).
+// fixed_of returns F and the sign of v.
 template <int S>
-__device__ __forceinline__ void slice_value(double v, int e, int8_t (&q)[S]) {
+__device__ __forceinline__ uint64_t fixed_of(double v, int e, bool& neg) {
   static_assert(S * 7 <= 63, "slices exceed a 64-bit fixed-point value");
   const uint64_t bits = (uint64_t)__double_as_longlong(v);
   const int E = (int)((bits >> 52) & 0x7ff);
   const uint64_t mant = bits & ((1ull << 52) - 1);
   const uint64_t M = E ? (mant | (1ull << 52)) : mant;
   const int sh = 7 * S - e + (E ? E : 1) - 1075;  // F = M * 2^sh
-  uint64_t F;
-  if (sh >= 0)
-    F = sh >= 64 ? 0 : (M << sh);  // |v| < 2^e bounds F below 2^(7 S)
-  else
-    F = -sh >= 64 ? 0 : (M >> -sh);
-  const bool neg = (bits >> 63) != 0;
-#pragma unroll
-  for (int t = 0; t < S; ++t) {
-    const int g = (int)((F >> (7 * (S - 1 - t))) & 127);
-    q[t] = (int8_t)(neg ? -g : g);
-  }
+  neg = (bits >> 63) != 0;
+  if (sh >= 0) return sh >= 64 ? 0 : (M << sh);  // |v| < 2^e bounds F below 2^(7 S)
+  return -sh >= 64 ? 0 : (M >> -sh);
 }
 
 // Fixed-point magnitudes of four values of a row (column) with exponent e:
@@ -97,6 +90,54 @@ __device__ __forceinline__ unsigned long long magnitude_fx4(const double (&v)[4]
 #pragma unroll
   for (int j = 0; j < 4; ++j) t += __double2ull_rz(ldexp(fabs(v[j]), 30 - e));
   return t;
+}
+
+// Bits [o, o + 7) of the 64-bit value hi:lo moved to bits [p, p + 7), all
+// other bits zero (o and p are constants once the callers' loops unroll:
+// one shift and one masked OR per digit).
+__device__ __forceinline__ uint32_t digit_at(uint32_t lo, uint32_t hi, int o, int p) {
+  const int n = o - p;
+  uint32_t x;
+  if (n >= 32)
+    x = hi >> (n - 32);
+  else if (n > 0)
+    x = __funnelshift_r(lo, hi, n);
+  else
+    x = lo << (-n);
+  return x & (127u << p);
+}
+
+// The slices of four values, packed: byte j of w[t] is slice_value's q_t of
+// v[j] (the 4-byte word the packed and stacked layouts store for four
+// consecutive k).  The digits of |v_j| are gathered into the word first and
+// the negative values' bytes negated together: per byte, 0x80 - g never
+// borrows for g <= 127, and (0x80 - g) ^ 0x80 = -g mod 256 (0 for g = 0).
+// Returns the magnitude sum of magnitude_fx4, from the same fixed-point
+// values when 7 S >= 30: floor(F 2^-(7S - 30)) = floor(|v| 2^(30 - e)).
+template <int S>
+__device__ __forceinline__ unsigned long long slice4_packed(const double (&v)[4], int e, uint32_t (&w)[S]) {
+  uint32_t lo[4], hi[4], nm = 0;
+  unsigned long long mag = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    bool neg;
+    const uint64_t F = fixed_of<S>(v[j], e, neg);
+    lo[j] = (uint32_t)F;
+    hi[j] = (uint32_t)(F >> 32);
+    nm |= neg ? 0xffu << (8 * j) : 0u;
+    if constexpr (7 * S >= 30) mag += F >> (7 * S - 30);
+  }
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    const int o = 7 * (S - 1 - t);
+    uint32_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x |= digit_at(lo[j], hi[j], o, 8 * j);
+    const uint32_t nx = (0x80808080u - x) ^ 0x80808080u;
+    w[t] = (x & ~nm) | (nx & nm);
+  }
+  if constexpr (7 * S < 30) mag = magnitude_fx4(v, e);
+  return mag;
 }
 
 // Packed slice layout shared by both operands: for row r (a row of A, or a
