@@ -365,24 +365,28 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// B (K x N) -> stacked slices of its columns, through a 32 (k) x 64 (n)
-// shared-memory tile.  Loads: 16 lanes cover 64 doubles of a row of B.
-// Stores: a lane slices 4 consecutive k of one column into one 4-byte store
-// per slice; 8 lanes cover a column's 32 bytes and a warp 4 adjacent columns
-// (128 contiguous bytes per slice).
+// B (K x N) -> stacked slices of its columns, through a 64 (k) x 64 (n)
+// shared-memory tile (two 32-wide k-blocks: eight 16-byte loads per thread
+// in flight before the barrier).  Loads: 16 lanes cover 64 doubles of a row
+// of B.  Stores, per k-block: a lane slices 4 consecutive k of one column
+// into one 4-byte store per slice; 8 lanes cover a column's 32 bytes and a
+// warp 4 adjacent columns (128 contiguous bytes per slice).  The second
+// k-block of the last tile may lie past kpad and is then skipped.
 // Also finishes the column exponents (the blocks of the first k-tile turn
 // the all-zero columns' sentinel into exp_of(0) = 0; every block reads the
 // sentinel as 0) and, with colsum, adds each column's fixed-point magnitude
 // sum sum_k floor(|b_kn| 2^(30 - e_n)) by integer atomics (exact, so the
 // totals do not depend on the order of the blocks).
+constexpr int kColTileK = 64;
+
 template <int S>
 __global__ void __launch_bounds__(256)
     ozaki_slice_cols_kernel(const double* __restrict__ B, int64_t ldb, int krows, int ncols, int64_t kpad,
                             int32_t* __restrict__ eb, int8_t* __restrict__ out, unsigned long long* __restrict__ colsum) {
-  __shared__ double tile[32][65];
-  const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 64, t = threadIdx.x;
+  __shared__ double tile[kColTileK][65];
+  const int k0 = blockIdx.y * kColTileK, n0 = blockIdx.x * 64, t = threadIdx.x;
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
+  for (int p = 0; p < kColTileK / 16; ++p) {
     const int i = p * 16 + t / 16, c = (t % 16) * 4;
     const int k = k0 + i, n = n0 + c;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -402,19 +406,19 @@ __global__ void __launch_bounds__(256)
   }
   __syncthreads();
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    const int item = p * 256 + t, nl = item / 8, kq = item % 8;
-    const int n = n0 + nl, k = k0 + kq * 4;
+  for (int p = 0; p < kColTileK / 16; ++p) {
+    const int half = p >> 1;  // k-block of the tile
+    const int item = (p & 1) * 256 + t, nl = item / 8, kq = item % 8;
+    const int n = n0 + nl, kl = half * 32 + kq * 4, k = k0 + kl;
+    if (k0 + half * 32 >= kpad) break;  // past the last k-block (uniform over the block)
     unsigned long long part = 0;
     if (n < ncols) {
       int e = eb[n];
       if (e == kExpSentinel) {
         e = 0;
-        if (blockIdx.y == 0 && kq == 0) eb[n] = 0;
+        if (blockIdx.y == 0 && kl == 0) eb[n] = 0;
       }
-      double v[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) v[j] = tile[kq * 4 + j][nl];
+      const double v[4] = {tile[kl][nl], tile[kl + 1][nl], tile[kl + 2][nl], tile[kl + 3][nl]};
       uint32_t w[S];
       const unsigned long long mg = slice4_packed<S>(v, e, w);
 #pragma unroll
@@ -518,7 +522,7 @@ cudaError_t launch_split_bf16(const float* A, int64_t lda, int rows, int cols, i
 template <int S>
 static cudaError_t prep_b_s(const double* B, int64_t ldb, int k, int n, int64_t kpad, int32_t* eb, int8_t* sb,
                             unsigned long long* colsum, cudaStream_t st) {
-  dim3 grid((unsigned)ceil_div(n, 64), (unsigned)ceil_div(kpad, 32));
+  dim3 grid((unsigned)ceil_div(n, 64), (unsigned)ceil_div(kpad, kColTileK));
   ozaki_slice_cols_kernel<S><<<grid, 256, 0, st>>>(B, ldb, k, n, kpad, eb, sb, colsum);
   return cudaGetLastError();
 }
