@@ -91,6 +91,14 @@ static Tiling make_tiling(const Plan& pl, int slices, int bn, const cucosma_gemm
   int64_t splits = d->split_k > 0 ? d->split_k : 1;
   if (d->split_k <= 0 && tiles < slots) splits = std::max<int64_t>(1, std::min<int64_t>(slots / tiles, t.kblocks / 16));
   splits = std::max(splits, min_splits);
+  // More splits than one wave of units (the Ozaki exactness bound on long
+  // K): as many splits as the same number of waves holds, so that the last
+  // wave is full and every unit is shorter (256 x 256 x 1,048,576 at 8
+  // slices: 64 splits x 8 tiles = 3.5 waves of 148; 74 splits fill 4).
+  if (d->split_k <= 0 && splits > 1 && tiles * splits > slots) {
+    const int64_t waves = ceil_div(tiles * splits, (int64_t)slots);
+    splits = std::max(splits, waves * slots / tiles);
+  }
   splits = std::min<int64_t>(splits, t.kblocks);
   t.kb_per_split = (int)std::min<int64_t>(ceil_div(t.kblocks, splits), kbmax);
   t.splits = (int)ceil_div(t.kblocks, t.kb_per_split);

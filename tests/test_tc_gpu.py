@@ -441,6 +441,22 @@ def test_fused_split_forced_split_k(precision, ftile, utile):
     assert planf["splits"] == 5 and np.array_equal(outf, outu)
 
 
+def test_ozaki_long_k_splits_fill_whole_waves():
+    """At K = 1,048,576 exact INT32 diagonals need at least 64 splits (8
+    slices); the plan then takes as many splits as the same number of waves
+    of units holds, so the last wave is full: for 256 x 256 (8 tiles of
+    128 x 64) tiles x splits is a multiple of the SM count."""
+    import torch
+
+    A = torch.empty((256, 1048576), dtype=torch.float64, device="cuda")
+    B = torch.empty((1048576, 256), dtype=torch.float64, device="cuda")
+    Cm = torch.empty((256, 256), dtype=torch.float64, device="cuda")
+    plan = cc.get_plan(cc.make_desc(A, B, Cm, precision="ozaki", slices=8))
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    tiles = (256 // plan["tile_m"]) * (256 // plan["tile_n"])
+    assert plan["splits"] >= 64 and (tiles * plan["splits"]) % sms == 0, plan
+
+
 def test_fused_split_chosen_for_large_k():
     """Auto planning picks the fused kernel where the operands are read about
     once (256 x 256 x 262144, 256 x 262144 x 256) and not for a square
