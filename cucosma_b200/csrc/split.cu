@@ -168,14 +168,14 @@ __global__ void __launch_bounds__(256)
   if (c + 1 < ncols && m1 != 0.0) atomicMax(&eb[c + 1], exp_of(m1));
 }
 
-// A rows -> row exponents and packed slices: a 256-thread block per row.
-// Rows of up to kRowRegK columns are read once into registers (4 consecutive
-// columns per thread and step, two 16-byte loads), the maximum is reduced
-// across the block, and the slices are cut from the registers; longer rows
-// take a second pass over the row for the slices.  A thread's 4 columns give
-// one 4-byte store per slice.  With stats, also the row's magnitude sum
-// sum_k floor(|a_rk| 2^(30 - e_r)) (integer, so exact and order-free) enters
-// stats->min_row by atomicMin (zero rows stay out).
+// A rows of up to kRowRegK padded columns -> row exponents and packed
+// slices: a 256-thread block per row.  The row is read once into registers
+// (4 consecutive columns per thread and step, two 16-byte loads), the
+// maximum is reduced across the block, and the slices are cut from the
+// registers; a thread's 4 columns give one 4-byte store per slice.  With
+// rowsum, also the row's magnitude sum sum_k floor(|a_rk| 2^(30 - e_r))
+// (integer, so exact and order-free) into rowsum[r].  Longer rows take the
+// chunked kernels below.
 constexpr int kRowSteps = 8;                    // steps of 1024 columns held in registers
 constexpr int kRowRegK = kRowSteps * 1024;
 static_assert(kRowRegK == kOzakiRowChunk, "row chunk");
@@ -211,34 +211,21 @@ __global__ void __launch_bounds__(256)
   __shared__ double red[8];
   __shared__ unsigned long long red_sum[8];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool in_regs = kpad <= kRowRegK;
   for (int r = blockIdx.x; r < rows; r += gridDim.x) {
     const double* src = A + (int64_t)r * lda;
     double v[kRowSteps][4];
     double m = 0.0;
-    if (in_regs) {
 #pragma unroll
-      for (int j = 0; j < kRowSteps; ++j) {
-        const int c = (tid + 256 * j) * 4;
-        if (c < kpad) {
-          load4(src, c, cols, v[j]);
-        } else {
+    for (int j = 0; j < kRowSteps; ++j) {
+      const int c = (tid + 256 * j) * 4;
+      if (c < kpad) {
+        load4(src, c, cols, v[j]);
+      } else {
 #pragma unroll
-          for (int q = 0; q < 4; ++q) v[j][q] = 0.0;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(v[j][q]));
+        for (int q = 0; q < 4; ++q) v[j][q] = 0.0;
       }
-    } else {
-      // long rows: four steps' loads in flight per thread (the row is read
-      // twice, so this pass and the slicing pass below stream from HBM)
-#pragma unroll 4
-      for (int c = tid * 4; c < kpad; c += 1024) {
-        double w[4];
-        load4(src, c, cols, w);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) m = fmax(m, fabs(w[q]));
-      }
+      for (int q = 0; q < 4; ++q) m = fmax(m, fabs(v[j][q]));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -251,21 +238,11 @@ __global__ void __launch_bounds__(256)
     const int e = exp_of(m);
     if (tid == 0) ea[r] = e;
     unsigned long long sum = 0;
-    if (in_regs) {
 #pragma unroll
-      for (int j = 0; j < kRowSteps; ++j) {
-        const int c = (tid + 256 * j) * 4;
-        if (c < kpad) {
-          const unsigned long long mg = store_slices4<S>(out, r, c, kpad, v[j], e);
-          if (stats) sum += mg;
-        }
-      }
-    } else {
-#pragma unroll 4
-      for (int c = tid * 4; c < kpad; c += 1024) {
-        double w[4];
-        load4(src, c, cols, w);
-        const unsigned long long mg = store_slices4<S>(out, r, c, kpad, w, e);
+    for (int j = 0; j < kRowSteps; ++j) {
+      const int c = (tid + 256 * j) * 4;
+      if (c < kpad) {
+        const unsigned long long mg = store_slices4<S>(out, r, c, kpad, v[j], e);
         if (stats) sum += mg;
       }
     }
