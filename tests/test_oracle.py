@@ -140,3 +140,66 @@ def test_ozaki_alpha_beta():
     Cin = uniform(18, (10, 9), np.float64)
     out = oracle.ozaki_gemm(A, B, 9, Cin=Cin, alpha=2.0, beta=0.5)
     np.testing.assert_allclose(out, 2.0 * (A @ B) + 0.5 * Cin, rtol=1e-13, atol=1e-14)
+
+
+def _packed_slice_words(row, e, s):
+    """Python statement of the device's packed slicing (split_device.cuh,
+    fixed_of / digit_at / slice4_packed): per 4 consecutive values, the
+    fixed-point F = floor(|v| 2^(7s - e)) from the FP64 bits, digit t of
+    value j shifted into byte j of word t, the negative values' bytes negated
+    as (0x80808080 - w) ^ 0x80808080, and the magnitude sum F >> (7s - 30)."""
+    import struct
+
+    m32 = 0xFFFFFFFF
+    words, mags = [], []
+    for c in range(0, len(row), 4):
+        lo, hi, nm, mag = [], [], 0, 0
+        for j, v in enumerate(row[c:c + 4]):
+            bits = struct.unpack("<Q", struct.pack("<d", float(v)))[0]
+            ex, mant = (bits >> 52) & 0x7FF, bits & ((1 << 52) - 1)
+            sig = (mant | (1 << 52)) if ex else mant
+            sh = 7 * s - e + (ex if ex else 1) - 1075
+            f = (0 if sh >= 64 else (sig << sh) & ((1 << 64) - 1)) if sh >= 0 else (0 if -sh >= 64 else sig >> -sh)
+            lo.append(f & m32)
+            hi.append(f >> 32)
+            if bits >> 63:
+                nm |= 0xFF << (8 * j)
+            mag += f >> (7 * s - 30) if 7 * s >= 30 else 0
+        row_words = []
+        for t in range(s):
+            o, x = 7 * (s - 1 - t), 0
+            for j in range(4):
+                n = o - 8 * j
+                y = hi[j] >> (n - 32) if n >= 32 else (((hi[j] << 32 | lo[j]) >> n) & m32 if n > 0 else (lo[j] << -n) & m32)
+                x |= y & (127 << (8 * j))
+            nx = ((0x80808080 - x) & m32) ^ 0x80808080
+            row_words.append((x & ~nm & m32) | (nx & nm))
+        words.append(row_words)
+        mags.append(mag)
+    return words, mags
+
+
+@pytest.mark.parametrize("s", [4, 5, 6, 7, 8, 9])
+def test_packed_slice_words_match_the_slicing(s):
+    """The word-at-a-time slicing of the device pre-passes gives, byte for
+    byte, the restatement's slices (the FP64 truncation sequence), and its
+    magnitude sums equal ozaki_magnitude_sums: rows with wide exponent
+    ranges, negative and signed-zero entries, subnormals and a zero row."""
+    rng = np.random.default_rng(40 + s)
+    m, k = 12, 32
+    A = rng.uniform(-1, 1, (m, k)) * 10.0 ** rng.integers(-30, 30, (m, k))
+    A[1, ::3] = -0.0
+    A[2] = 0.0
+    A[3] = rng.uniform(-1, 1, k) * 1e-310  # subnormal row
+    A[4, 5] = 1e300
+    B = np.ones((k, 1))
+    ea, _, sa, _ = oracle.ozaki_slices(A, B, s)
+    rows_sums, _ = oracle.ozaki_magnitude_sums(A, B)
+    for r in range(m):
+        words, mags = _packed_slice_words(A[r], int(ea[r]), s)
+        for g, row_words in enumerate(words):
+            for t, w in enumerate(row_words):
+                expect = bytes(sa[t, r, 4 * g:4 * g + 4].view(np.uint8))
+                assert w.to_bytes(4, "little") == expect, (r, g, t)
+        if 7 * s >= 30:
+            assert sum(mags) == rows_sums[r]
